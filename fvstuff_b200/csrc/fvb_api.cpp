@@ -1,0 +1,613 @@
+// fvb_api.cpp -- the single-grid solver behind the C ABI (include/fvb.h).
+//
+// A solver owns one device allocation holding its padded state buffers, the
+// two stage buffers and its step control.  fvb_step enqueues three stage
+// launches per step (or replays them as a CUDA graph) and never waits;
+// dt, the CFL reduction and the stop test all live on the device, so the
+// host synchronises only when it asks for the state or the step control.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fvb_aux.h"
+#include "fvb_host.h"
+
+namespace fvb {
+
+thread_local std::string g_err;
+
+fvb_status fail(fvb_status st, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return st;
+}
+
+fvb_status cuda_fail(cudaError_t e, const char *what)
+{
+    return fail(FVB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int prec_internal(int prec)
+{
+    return prec == FVB_PREC_F64 ? INT_PRIM64 : prec == FVB_PREC_F32 ? INT_PRIM32 : INT_CONS_HILO;
+}
+
+size_t prec_elem(int prec) { return prec == FVB_PREC_F64 ? 8 : 4; }
+
+Geometry make_geometry(int n, int g, int prec)
+{
+    Geometry G{};
+    const int align = 16;  // interior rows start 16 elements into a 16-aligned row
+    G.n = n;
+    G.g = g;
+    G.np = n + 2 * g;
+    G.xoff = align - g;
+    G.pitch = ((G.xoff + G.np + align - 1) / align) * align;
+    G.plane = (((long long)G.pitch * G.np + 63) / 64) * 64;
+    G.elem = prec_elem(prec);
+    G.nbuf = prec == FVB_PREC_F32C ? 6 : 3;
+    G.bytes = (size_t)G.nbuf * 4 * G.plane * G.elem;
+    return G;
+}
+
+void grid_pointers(GridDev &gd, void *base, const Geometry &G, int prec)
+{
+    char *p = (char *)base;
+    size_t bb = (size_t)4 * G.plane * G.elem;
+    gd.n = G.n;
+    gd.g = G.g;
+    gd.pitch = G.pitch;
+    gd.xoff = G.xoff;
+    gd.plane = G.plane;
+    if (prec == FVB_PREC_F32C) {
+        gd.st[0] = p; gd.st[1] = p + bb; gd.lo[0] = p + 2 * bb; gd.lo[1] = p + 3 * bb;
+        gd.k1 = p + 4 * bb; gd.k2 = p + 5 * bb;
+    } else {
+        gd.st[0] = p; gd.st[1] = nullptr; gd.lo[0] = gd.lo[1] = nullptr;
+        gd.k1 = p + bb; gd.k2 = p + 2 * bb;
+    }
+}
+
+BufView view_of(const GridDev &gd) { return BufView{gd.n, gd.g, gd.pitch, gd.xoff, gd.plane}; }
+
+void tile_dims(int shape, int n, int &tiles_x, int &tiles)
+{
+    const TileShape &t = kTileShapes[shape];
+    tiles_x = (n + t.tx - 1) / t.tx;
+    tiles = tiles_x * ((n + t.ty - 1) / t.ty);
+}
+
+void case_defaults(fvb_case *c, int kind, double x0, double y0, double L)
+{
+    std::memset(c, 0, sizeof *c);
+    c->kind = kind;
+    switch (kind) {
+    case FVB_CASE_SOD:
+        c->param[0] = x0 + 0.5 * L; c->param[1] = y0 + 0.5 * L; c->param[2] = 0.25 * L;
+        c->param[3] = 0.125; c->param[4] = 11.0; c->param[5] = 0.1; c->param[6] = 10.0;
+        break;
+    case FVB_CASE_VORTEX:
+        c->param[0] = 5.0; c->param[1] = 1.0; c->param[2] = 1.0;
+        c->param[3] = x0 + 0.5 * L; c->param[4] = y0 + 0.5 * L;
+        break;
+    case FVB_CASE_KH:
+        c->param[0] = y0 + 0.5 * L; c->param[1] = 0.25 * L; c->param[2] = 2.0; c->param[3] = 1.0;
+        c->param[4] = -0.5; c->param[5] = 0.5; c->param[6] = 2.5; c->param[7] = 1e-3;
+        c->seed = 12345;
+        break;
+    case FVB_CASE_RIEMANN4:
+        c->param[0] = x0 + 0.5 * L; c->param[1] = y0 + 0.5 * L;
+        c->seed = 1;
+        break;
+    case FVB_CASE_LMV:
+        c->param[0] = 0.1;
+        break;
+    case FVB_CASE_UNIFORM:
+        c->param[0] = 1.0; c->param[3] = 1.0;
+        break;
+    default:
+        break;
+    }
+}
+
+}  // namespace fvb
+
+using namespace fvb;
+
+struct fvb_solver {
+    fvb_config cfg;
+    int prec = 0, order = 7, g = 4, n = 0;
+    int internal = 0;
+    Geometry G{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    void *block = nullptr;
+    GridDev gd{};
+    Ctrl *ctrl = nullptr;       // device
+    Ctrl *ctrl_host = nullptr;  // pinned
+    void *staging = nullptr;    // device, 4 (n+2g)^2 doubles
+    double *sums_dev = nullptr, *sums_host = nullptr;
+    int sums_blocks = 0;
+    int shape = 0, tiles = 0, ctas = 0;
+    int parity = 0;
+    bool use_graph = false;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int graph_steps = 1;
+};
+
+static fvb_status ensure_staging(fvb_solver *s)
+{
+    if (s->staging) return FVB_OK;
+    size_t bytes = (size_t)4 * s->G.np * s->G.np * sizeof(double);
+    cudaError_t e = cudaMalloc(&s->staging, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(staging)");
+    return FVB_OK;
+}
+
+static StageArgs stage_args(const fvb_solver *s, int stage, int parity)
+{
+    StageArgs a{};
+    a.grid = s->gd;
+    a.grids = nullptr;
+    a.tiles = nullptr;
+    a.ntiles = nullptr;
+    a.ntiles_static = s->tiles;
+    a.stage = stage;
+    a.parity = parity;
+    return a;
+}
+
+static cudaError_t enqueue_steps_direct(fvb_solver *s, int nsteps)
+{
+    for (int k = 0; k < nsteps; ++k) {
+        for (int stage = 1; stage <= 3; ++stage) {
+            StageArgs a = stage_args(s, stage, s->parity);
+            cudaError_t e = launch_stage(s->prec, s->order, s->shape, a, s->ctas, s->stream);
+            if (e != cudaSuccess) return e;
+        }
+        if (s->prec == FVB_PREC_F32C) s->parity ^= 1;
+    }
+    return cudaSuccess;
+}
+
+static void drop_graphs(fvb_solver *s)
+{
+    for (auto &g : s->gexec)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+static cudaError_t capture_graph(fvb_solver *s, int parity)
+{
+    cudaGraph_t graph = nullptr;
+    int saved = s->parity;
+    s->parity = parity;
+    cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) { s->parity = saved; return e; }
+    cudaError_t el = enqueue_steps_direct(s, s->graph_steps);
+    e = cudaStreamEndCapture(s->stream, &graph);
+    s->parity = saved;
+    if (el != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return el; }
+    if (e != cudaSuccess) return e;
+    e = cudaGraphInstantiate(&s->gexec[parity], graph, 0);
+    cudaGraphDestroy(graph);
+    return e;
+}
+
+static cudaError_t enqueue_steps(fvb_solver *s, int nsteps)
+{
+    if (!s->use_graph) return enqueue_steps_direct(s, nsteps);
+    while (nsteps >= s->graph_steps) {
+        int p = s->parity;
+        if (!s->gexec[p]) {
+            cudaError_t e = capture_graph(s, p);
+            if (e != cudaSuccess) return e;
+        }
+        cudaError_t e = cudaGraphLaunch(s->gexec[p], s->stream);
+        if (e != cudaSuccess) return e;
+        nsteps -= s->graph_steps;
+        // a graph of an even number of F32C steps ends on its start parity
+    }
+    return enqueue_steps_direct(s, nsteps);
+}
+
+static fvb_status refresh_after_state(fvb_solver *s, int buf_parity)
+{
+    cudaError_t e;
+    BufView v = view_of(s->gd);
+    if (s->internal == INT_PRIM64) e = bc_fill<double>((double *)s->gd.st[0], v, s->gd.bcx, s->gd.bcy, s->stream);
+    else if (s->internal == INT_PRIM32) e = bc_fill<float>((float *)s->gd.st[0], v, s->gd.bcx, s->gd.bcy, s->stream);
+    else {
+        e = bc_fill<float>((float *)s->gd.st[buf_parity], v, s->gd.bcx, s->gd.bcy, s->stream);
+        if (e == cudaSuccess) e = bc_fill<float>((float *)s->gd.lo[buf_parity], v, s->gd.bcx, s->gd.bcy, s->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "ghost fill");
+    e = lam_into(s->gd.st[s->internal == INT_CONS_HILO ? buf_parity : 0], v, s->internal, s->cfg.gamma,
+                 &s->ctrl->lam_acc, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "max wave speed");
+    e = ctrl_set(s->ctrl, 0.0, 1, 0.0, s->cfg.cfl, s->cfg.length / s->n, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "step control reset");
+    return FVB_OK;
+}
+
+extern "C" {
+
+const char *fvb_version(void) { return "fvb 0.1 (sm_100a)"; }
+
+const char *fvb_last_error(void) { return g_err.c_str(); }
+
+void fvb_config_default(fvb_config *c, int n)
+{
+    std::memset(c, 0, sizeof *c);
+    c->n = n;
+    c->order = 7;
+    c->flux = FVB_FLUX_UP_DUCROS;
+    c->precision = FVB_PREC_F64;
+    c->bc_x = c->bc_y = FVB_BC_REFLECT;
+    c->x0 = 0.0;
+    c->y0 = 0.0;
+    c->length = 1.0;
+    c->gamma = 1.4;
+    c->cfl = 0.4;
+    c->device = 0;
+    c->stream = nullptr;
+    c->tile = -1;
+}
+
+void fvb_case_default(fvb_case *c, int kind, double x0, double y0, double length)
+{
+    case_defaults(c, kind, x0, y0, length);
+}
+
+fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
+{
+    if (!cfg || !out) return fail(FVB_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (cfg->flux == FVB_FLUX_KEEP) return keep_create(cfg, out);
+    if (cfg->flux != FVB_FLUX_UP_DUCROS) return fail(FVB_ERR_INVALID, "unknown flux %d", cfg->flux);
+    if (cfg->precision < 0 || cfg->precision > 2) return fail(FVB_ERR_INVALID, "unknown precision %d", cfg->precision);
+    if (!(cfg->order == 3 || cfg->order == 5 || cfg->order == 7))
+        return fail(FVB_ERR_INVALID, "order must be 3, 5 or 7 (got %d)", cfg->order);
+    if (cfg->precision != FVB_PREC_F64 && cfg->order != 7)
+        return fail(FVB_ERR_INVALID, "orders 3 and 5 are built for FP64 only");
+    const int g = (cfg->order + 1) / 2;
+    if (cfg->n < g || cfg->n > 65536) return fail(FVB_ERR_INVALID, "n = %d out of range [%d, 65536]", cfg->n, g);
+    for (int b : {cfg->bc_x, cfg->bc_y})
+        if (b < 0 || b > 2) return fail(FVB_ERR_INVALID, "unknown boundary condition %d", b);
+    if (!(cfg->length > 0) || !(cfg->cfl > 0) || !(cfg->gamma > 1))
+        return fail(FVB_ERR_INVALID, "length, cfl must be > 0 and gamma > 1");
+    if (cfg->tile >= kNumTileShapes) return fail(FVB_ERR_INVALID, "tile variant %d out of range", cfg->tile);
+
+    cudaError_t e = cudaSetDevice(cfg->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+
+    fvb_solver *s = new fvb_solver();
+    s->cfg = *cfg;
+    s->prec = cfg->precision;
+    s->order = cfg->order;
+    s->g = g;
+    s->n = cfg->n;
+    s->internal = prec_internal(s->prec);
+    s->G = make_geometry(cfg->n, g, s->prec);
+    if (cfg->stream) s->stream = (cudaStream_t)cfg->stream;
+    else {
+        e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaStreamCreate"); }
+        s->own_stream = true;
+    }
+    size_t total = s->G.bytes + 256;
+    e = cudaMalloc(&s->block, total);
+    if (e != cudaSuccess) {
+        fvb_destroy(s);
+        return fail(FVB_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", total, cudaGetErrorString(e));
+    }
+    e = cudaMemsetAsync(s->block, 0, total, s->stream);
+    if (e != cudaSuccess) { fvb_destroy(s); return cuda_fail(e, "cudaMemset"); }
+    grid_pointers(s->gd, s->block, s->G, s->prec);
+    s->ctrl = (Ctrl *)((char *)s->block + s->G.bytes);
+    s->gd.ctrl = s->ctrl;
+    s->gd.bcx = cfg->bc_x;
+    s->gd.bcy = cfg->bc_y;
+    s->gd.h = cfg->length / cfg->n;
+    s->gd.gam = cfg->gamma;
+    e = cudaMallocHost(&s->ctrl_host, sizeof(Ctrl));
+    if (e != cudaSuccess) { fvb_destroy(s); return cuda_fail(e, "cudaMallocHost"); }
+
+    s->shape = cfg->tile >= 0 ? cfg->tile : autotune_shape(s->prec, s->order, cfg->n);
+    tile_dims(s->shape, s->n, s->gd.tiles_x, s->tiles);
+    s->ctas = s->tiles;
+    s->graph_steps = s->prec == FVB_PREC_F32C ? 2 : 1;
+    s->use_graph = cfg->n <= 512;
+    e = ctrl_set(s->ctrl, 0.0, 1, 0.0, cfg->cfl, s->gd.h, s->stream);
+    if (e != cudaSuccess) { fvb_destroy(s); return cuda_fail(e, "step control"); }
+    // make sure the kernel variant can launch on this device
+    if (stage_max_ctas_per_sm(s->prec, s->order, s->shape) <= 0) {
+        fvb_destroy(s);
+        return fail(FVB_ERR_CUDA, "stage kernel variant cannot be resident on this device");
+    }
+    *out = s;
+    return FVB_OK;
+}
+
+void fvb_destroy(fvb_solver *s)
+{
+    if (!s) return;
+    if (s->cfg.flux == FVB_FLUX_KEEP) { keep_destroy(s); return; }
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    drop_graphs(s);
+    if (s->block) cudaFree(s->block);
+    if (s->staging) cudaFree(s->staging);
+    if (s->sums_dev) cudaFree(s->sums_dev);
+    if (s->sums_host) cudaFreeHost(s->sums_host);
+    if (s->ctrl_host) cudaFreeHost(s->ctrl_host);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+int fvb_ghost_width(const fvb_solver *s) { return s ? s->g : 0; }
+
+fvb_status fvb_init_case(fvb_solver *s, const fvb_case *c)
+{
+    if (!s || !c) return fail(FVB_ERR_INVALID, "null argument");
+    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_init_case(s, c);
+    fvb_status st = ensure_staging(s);
+    if (st) return st;
+    cudaError_t e = init_case_prim64((double *)s->staging, s->n, s->cfg.x0, s->cfg.y0, s->gd.h, s->cfg.gamma, *c,
+                                     s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "initial state");
+    ExtView ev{1, s->g, s->G.np, FVB_LAYOUT_PRIM, FVB_F64};
+    int p = s->parity;
+    e = import_state(s->staging, ev, s->gd.st[s->internal == INT_CONS_HILO ? p : 0], s->gd.lo[p], view_of(s->gd),
+                     s->internal, s->cfg.gamma, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "import");
+    return refresh_after_state(s, p);
+}
+
+fvb_status fvb_set_state(fvb_solver *s, const void *src, int layout, int dtype, int where, int interior_only)
+{
+    if (!s || !src) return fail(FVB_ERR_INVALID, "null argument");
+    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_set_state(s, src, layout, dtype, where, interior_only);
+    if ((layout != 0 && layout != 1) || (dtype != 0 && dtype != 1) || (where != 0 && where != 1))
+        return fail(FVB_ERR_INVALID, "bad layout/dtype/where");
+    ExtView ev{interior_only ? 1 : 0, s->g, s->G.np, layout, dtype};
+    const void *dev = src;
+    if (where == FVB_HOST) {
+        fvb_status st = ensure_staging(s);
+        if (st) return st;
+        long long side = interior_only ? s->n : s->G.np;
+        size_t bytes = (size_t)4 * side * side * (dtype == FVB_F64 ? 8 : 4);
+        cudaError_t e = cudaMemcpyAsync(s->staging, src, bytes, cudaMemcpyHostToDevice, s->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "copy in");
+        dev = s->staging;
+    }
+    int p = s->parity;
+    cudaError_t e = import_state(dev, ev, s->gd.st[s->internal == INT_CONS_HILO ? p : 0], s->gd.lo[p],
+                                 view_of(s->gd), s->internal, s->cfg.gamma, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "import");
+    fvb_status st = refresh_after_state(s, p);
+    if (st) return st;
+    if (where == FVB_HOST) {
+        e = cudaStreamSynchronize(s->stream);  // the caller may reuse its buffer on return
+        if (e != cudaSuccess) return cuda_fail(e, "sync");
+    }
+    return FVB_OK;
+}
+
+fvb_status fvb_get_state(fvb_solver *s, void *dst, int layout, int dtype, int where, int interior_only)
+{
+    if (!s || !dst) return fail(FVB_ERR_INVALID, "null argument");
+    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_get_state(s, dst, layout, dtype, where, interior_only);
+    if ((layout != 0 && layout != 1) || (dtype != 0 && dtype != 1) || (where != 0 && where != 1))
+        return fail(FVB_ERR_INVALID, "bad layout/dtype/where");
+    ExtView ev{interior_only ? 1 : 0, s->g, s->G.np, layout, dtype};
+    void *dev = dst;
+    if (where == FVB_HOST) {
+        fvb_status st = ensure_staging(s);
+        if (st) return st;
+        dev = s->staging;
+    }
+    int p = s->parity;
+    cudaError_t e = export_state(s->gd.st[s->internal == INT_CONS_HILO ? p : 0], s->gd.lo[p], view_of(s->gd),
+                                 s->internal, dev, ev, s->cfg.gamma, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "export");
+    if (where == FVB_HOST) {
+        long long side = interior_only ? s->n : s->G.np;
+        size_t bytes = (size_t)4 * side * side * (dtype == FVB_F64 ? 8 : 4);
+        e = cudaMemcpyAsync(dst, s->staging, bytes, cudaMemcpyDeviceToHost, s->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "copy out");
+        e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "sync");
+    }
+    return FVB_OK;
+}
+
+fvb_status fvb_get_state_hilo(fvb_solver *s, float *hi, float *lo)
+{
+    if (!s || !hi || !lo) return fail(FVB_ERR_INVALID, "null argument");
+    if (s->internal != INT_CONS_HILO) return fail(FVB_ERR_INVALID, "solver is not in the compensated FP32 mode");
+    size_t row = (size_t)s->n * sizeof(float);
+    int p = s->parity;
+    for (int q = 0; q < 4; ++q) {
+        size_t off = ((size_t)q * s->G.plane + (size_t)s->g * s->G.pitch + s->g + s->G.xoff) * sizeof(float);
+        cudaError_t e = cudaMemcpy2DAsync(hi + (size_t)q * s->n * s->n, row, (char *)s->gd.st[p] + off,
+                                          s->G.pitch * sizeof(float), row, s->n, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(lo + (size_t)q * s->n * s->n, row, (char *)s->gd.lo[p] + off,
+                                  s->G.pitch * sizeof(float), row, s->n, cudaMemcpyDeviceToHost, s->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "copy out");
+    }
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    return e == cudaSuccess ? FVB_OK : cuda_fail(e, "sync");
+}
+
+fvb_status fvb_step(fvb_solver *s, int nsteps, double t_stop)
+{
+    if (!s || nsteps < 0) return fail(FVB_ERR_INVALID, "bad argument");
+    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_step(s, nsteps, t_stop);
+    cudaError_t e = ctrl_set(s->ctrl, t_stop, 0, 0, 0, 0, s->stream);
+    if (e == cudaSuccess) e = enqueue_steps(s, nsteps);
+    if (e != cudaSuccess) return cuda_fail(e, "step launch");
+    return FVB_OK;
+}
+
+fvb_status fvb_sync(fvb_solver *s, fvb_stats *st)
+{
+    if (!s) return fail(FVB_ERR_INVALID, "null solver");
+    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_sync(s, st);
+    cudaError_t e = cudaMemcpyAsync(s->ctrl_host, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "sync");
+    if (st) {
+        std::memset(st, 0, sizeof *st);
+        const Ctrl &c = *s->ctrl_host;
+        st->t = c.t;
+        st->dt = c.dt;
+        unsigned long long b = c.lam_acc;
+        std::memcpy(&st->lam_max, &b, sizeof b);
+        st->t_stop = c.t_stop;
+        st->steps = c.step;
+        st->status = c.status;
+    }
+    return FVB_OK;
+}
+
+fvb_status fvb_advance(fvb_solver *s, double t_stop, int64_t max_steps, int chunk)
+{
+    if (!s) return fail(FVB_ERR_INVALID, "null solver");
+    int64_t done = 0;
+    for (;;) {
+        fvb_stats st;
+        fvb_status r = fvb_sync(s, &st);
+        if (r) return r;
+        if (st.status) return fail((fvb_status)st.status, "step control stopped at t=%.9g step %lld (%s)", st.t,
+                                   (long long)st.steps, st.status == FVB_ERR_BLOWUP ? "lam_max not > 0" : "dt underflow");
+        if (!(st.t < t_stop) || done >= max_steps) return FVB_OK;
+        int64_t k = chunk;
+        if (k <= 0) {
+            double dt = st.lam_max > 0 ? s->cfg.cfl * (s->cfg.length / s->n) / st.lam_max : 0;
+            double est = dt > 0 ? (t_stop - st.t) / dt : 1e9;
+            k = (int64_t)std::min(est * 1.05 + 2.0, 4096.0);
+            if (k < 1) k = 1;
+        }
+        if (k > max_steps - done) k = max_steps - done;
+        r = fvb_step(s, (int)k, t_stop);
+        if (r) return r;
+        done += k;
+    }
+}
+
+fvb_status fvb_stats_sums(fvb_solver *s, fvb_stats *st)
+{
+    if (!s || !st) return fail(FVB_ERR_INVALID, "null argument");
+    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_stats_sums(s, st);
+    if (!s->sums_dev) {
+        s->sums_blocks = 592;
+        cudaError_t e = cudaMalloc(&s->sums_dev, sizeof(double) * 5 * s->sums_blocks);
+        if (e == cudaSuccess) e = cudaMallocHost(&s->sums_host, sizeof(double) * 5 * s->sums_blocks);
+        if (e != cudaSuccess) return cuda_fail(e, "sums buffers");
+    }
+    int p = s->parity;
+    cudaError_t e = sums_partials(s->gd.st[s->internal == INT_CONS_HILO ? p : 0], s->gd.lo[p], view_of(s->gd),
+                                  s->internal, s->cfg.gamma, s->sums_dev, s->sums_blocks, s->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->sums_host, s->sums_dev, sizeof(double) * 5 * s->sums_blocks, cudaMemcpyDeviceToHost,
+                            s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "sums");
+    fvb_status r = fvb_sync(s, st);
+    if (r) return r;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int b = 0; b < s->sums_blocks; ++b)
+        for (int q = 0; q < 5; ++q) acc[q] += s->sums_host[b * 5 + q];
+    double h2 = s->gd.h * s->gd.h;
+    for (int q = 0; q < 4; ++q) st->sums[q] = acc[q] * h2;
+    st->nonfinite = acc[4] > 0;
+    return FVB_OK;
+}
+
+fvb_status fvb_set_graph(fvb_solver *s, int enable)
+{
+    if (!s) return fail(FVB_ERR_INVALID, "null solver");
+    if (s->cfg.flux == FVB_FLUX_KEEP) return FVB_OK;
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "sync");
+    s->use_graph = enable != 0;
+    if (!s->use_graph) drop_graphs(s);
+    return FVB_OK;
+}
+
+// ---- kernel-level contract ---------------------------------------------
+
+fvb_status fvb_up_rhs(const void *Qp, void *rhs, void *lam, int n, int np, int order, double h, double gamma,
+                      int dtype, void *stream)
+{
+    if (!Qp || !rhs || !lam) return fail(FVB_ERR_INVALID, "null argument");
+    if (order != 7 && !(dtype == FVB_F64 && (order == 3 || order == 5)))
+        return fail(FVB_ERR_INVALID, "order %d not built for this dtype", order);
+    const int g = (order + 1) / 2;
+    if (n < 1 || np < n + 2 * g) return fail(FVB_ERR_INVALID, "np must be >= n + 2g");
+    StageArgs a{};
+    GridDev &gd = a.grid;
+    gd.n = n;
+    gd.g = g;
+    gd.pitch = np;
+    gd.xoff = 0;
+    gd.plane = (long long)np * np;
+    gd.h = h;
+    gd.gam = gamma;
+    gd.st[0] = (void *)Qp;
+    gd.ctrl = nullptr;
+    const int shape = 0;
+    int tiles;
+    tile_dims(shape, n, gd.tiles_x, tiles);
+    a.ntiles_static = tiles;
+    a.stage = 0;
+    a.rhs = rhs;
+    a.lam = lam;
+    int prec = dtype == FVB_F64 ? P64 : P32;
+    cudaError_t e = launch_stage(prec, order, shape, a, tiles, (cudaStream_t)stream);
+    return e == cudaSuccess ? FVB_OK : cuda_fail(e, "fvb_up_rhs");
+}
+
+fvb_status fvb_apply_bc(void *Qp, int n, int np, int bc_x, int bc_y, int layout, int dtype, void *stream)
+{
+    if (!Qp) return fail(FVB_ERR_INVALID, "null argument");
+    if (np < n || (np - n) % 2 || bc_x < 0 || bc_x > 2 || bc_y < 0 || bc_y > 2 || (layout != 0 && layout != 1))
+        return fail(FVB_ERR_INVALID, "bad geometry or boundary condition");
+    BufView v{n, (np - n) / 2, np, 0, (long long)np * np};
+    if (v.g > n) return fail(FVB_ERR_INVALID, "ghost width exceeds n");
+    cudaError_t e = dtype == FVB_F64 ? bc_fill<double>((double *)Qp, v, bc_x, bc_y, (cudaStream_t)stream)
+                                     : bc_fill<float>((float *)Qp, v, bc_x, bc_y, (cudaStream_t)stream);
+    return e == cudaSuccess ? FVB_OK : cuda_fail(e, "fvb_apply_bc");
+}
+
+fvb_status fvb_rk3_stage(int stage, void *Uo, const void *U0, const void *Uk, const void *L, double dt, int n,
+                         int np, double gamma, int dtype, void *stream)
+{
+    if (!Uo || !U0 || !L || (stage != 1 && !Uk)) return fail(FVB_ERR_INVALID, "null argument");
+    if (stage < 1 || stage > 3 || np < n || (np - n) % 2) return fail(FVB_ERR_INVALID, "bad stage or geometry");
+    int g = (np - n) / 2;
+    cudaError_t e;
+    if (dtype == FVB_F64)
+        e = rk3_stage_ref<double>(stage, (double *)Uo, (const double *)U0, (const double *)Uk, (const double *)L, dt,
+                                  n, np, g, gamma, (cudaStream_t)stream);
+    else
+        e = rk3_stage_ref<float>(stage, (float *)Uo, (const float *)U0, (const float *)Uk, (const float *)L,
+                                 (float)dt, n, np, g, gamma, (cudaStream_t)stream);
+    return e == cudaSuccess ? FVB_OK : cuda_fail(e, "fvb_rk3_stage");
+}
+
+fvb_status fvb_max(const void *x, size_t n, void *out_dev, int dtype, void *stream)
+{
+    if (!x || !out_dev) return fail(FVB_ERR_INVALID, "null argument");
+    cudaError_t e = max_ref(x, n, out_dev, dtype, (cudaStream_t)stream);
+    return e == cudaSuccess ? FVB_OK : cuda_fail(e, "fvb_max");
+}
+
+}  // extern "C"

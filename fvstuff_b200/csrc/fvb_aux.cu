@@ -1,0 +1,504 @@
+// fvb_aux.cu -- the kernels around the stage kernel: ghost-ring fill,
+// initial states, layout conversion between the caller's IDX_P arrays and
+// the internal pitched buffers, the max-wave-speed reduction of a fresh
+// state, FP64 conserved sums, and the reference's pointwise kernels
+// (rk3_sX, reduce_max) for the kernel-level contract.
+#include <math.h>
+
+#include "fvb_aux.h"
+#include "fvb_physics.cuh"
+
+namespace fvb {
+
+// ---------------------------------------------------------------------------
+// ghost ring
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int src_coord(int p, int n, int g, int bc, bool &ghost)
+{
+    // padded coordinate p of a ghost -> padded coordinate of its source
+    ghost = (p < g || p >= n + g);
+    if (!ghost) return p;
+    if (bc == FVB_BC_REFLECT) return p < g ? 2 * g - 1 - p : 2 * (n + g) - 1 - p;
+    if (bc == FVB_BC_PERIODIC) return p < g ? p + n : p - n;
+    return p < g ? g : n + g - 1;
+}
+
+// Fill every ghost cell of a padded buffer from the interior cell it mirrors
+// (reflect: fv_up7_ducros_2d.cu:338-362, periodic: keep_fv_euler_2d.cu:224-243,
+// transmissive: zero-gradient).  One thread per ghost cell: the ring is
+// enumerated as the g bottom rows, the g top rows, then the left and right
+// g-wide column bands of the interior rows.
+template <class R>
+__global__ void bc_fill_kernel(R *buf, BufView v, int bcx, int bcy)
+{
+    const int n = v.n, g = v.g, np = n + 2 * g;
+    const long long band = (long long)g * np, side = (long long)g * n;
+    const long long total = 2 * band + 2 * side;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
+         k += (long long)blockDim.x * gridDim.x) {
+        int jp, ip;
+        if (k < band) { jp = (int)(k / np); ip = (int)(k % np); }
+        else if (k < 2 * band) { long long m = k - band; jp = n + g + (int)(m / np); ip = (int)(m % np); }
+        else {
+            long long m = k - 2 * band;
+            bool right = m >= side;
+            if (right) m -= side;
+            jp = g + (int)(m / g);
+            ip = (right ? n + g : 0) + (int)(m % g);
+        }
+        bool gx, gy;
+        int ir = src_coord(ip, n, g, bcx, gx), jr = src_coord(jp, n, g, bcy, gy);
+        long long d = (long long)jp * v.pitch + ip + v.xoff, s = (long long)jr * v.pitch + ir + v.xoff;
+        for (int q = 0; q < 4; ++q) {
+            R x = buf[s + q * v.plane];
+            if (q == 1 && gx && bcx == FVB_BC_REFLECT) x = -x;
+            if (q == 2 && gy && bcy == FVB_BC_REFLECT) x = -x;
+            buf[d + q * v.plane] = x;
+        }
+    }
+}
+
+template <class R>
+cudaError_t bc_fill(R *buf, const BufView &v, int bcx, int bcy, cudaStream_t s)
+{
+    long long total = 2LL * v.g * (v.n + 2 * v.g) + 2LL * v.g * v.n;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    bc_fill_kernel<R><<<blocks, 256, 0, s>>>(buf, v, bcx, bcy);
+    return cudaGetLastError();
+}
+template cudaError_t bc_fill<float>(float *, const BufView &, int, int, cudaStream_t);
+template cudaError_t bc_fill<double>(double *, const BufView &, int, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// initial states: primitives in FP64 into a (4, n, n) staging array
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// uniform in [0, 1) from the k-th draw of the stream `seed`
+__device__ __forceinline__ double unit_draw(uint64_t seed, uint64_t k)
+{
+    return (double)(splitmix64(seed * 0x9E3779B97F4A7C15ull + k) >> 11) * 0x1.0p-53;
+}
+
+__global__ void ic_kernel(double *out, int n, double x0, double y0, double h, double gam, fvb_case c)
+{
+    const long long n2 = (long long)n * n;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
+         k += (long long)blockDim.x * gridDim.x) {
+        const int j = (int)(k / n), i = (int)(k % n);
+        const double x = x0 + (i + 0.5) * h, y = y0 + (j + 0.5) * h;
+        double r = 1, u = 0, v = 0, p = 1;
+        switch (c.kind) {
+        case FVB_CASE_SOD: {
+            // circular Sod, tanh-smoothed over one cell (fv_up7_ducros_2d.cu:629-637)
+            double rr = sqrt((x - c.param[0]) * (x - c.param[0]) + (y - c.param[1]) * (y - c.param[1]));
+            double phi = 0.5 * (1. + tanh((c.param[2] - rr) / (1.0 * h)));
+            r = c.param[3] + (c.param[4] - c.param[3]) * phi;
+            p = c.param[5] + (c.param[6] - c.param[5]) * phi;
+            break;
+        }
+        case FVB_CASE_VORTEX: {
+            // isentropic vortex with mean flow (rt_dg_euler_2d.cu:1334-1356)
+            const double beta = c.param[0], pi = 3.14159265358979323846;
+            double dx = x - c.param[3], dy = y - c.param[4], r2 = dx * dx + dy * dy;
+            double f = beta / (2. * pi) * exp(0.5 * (1. - r2));
+            double T = 1. - (gam - 1.) * beta * beta / (8. * gam * pi * pi) * exp(1. - r2);
+            if (T < 1e-6) T = 1e-6;
+            r = pow(T, 1. / (gam - 1.));
+            p = pow(T, gam / (gam - 1.));
+            u = c.param[1] - f * dy;
+            v = c.param[2] + f * dx;
+            break;
+        }
+        case FVB_CASE_KH: {
+            // double shear layer: rho_in / u_in for |y - yc| < w, seeded noise on v
+            bool in = fabs(y - c.param[0]) < c.param[1];
+            r = in ? c.param[2] : c.param[3];
+            u = in ? c.param[4] : c.param[5];
+            p = c.param[6];
+            const double pi = 3.14159265358979323846;
+            double noise = 2. * unit_draw(c.seed, (uint64_t)k) - 1.;
+            v = 0.01 * sin(4. * pi * (x - x0) / (h * n)) + c.param[7] * noise;
+            break;
+        }
+        case FVB_CASE_RIEMANN4: {
+            // quadrant q = (x >= xm) + 2 (y >= ym); draws 4q..4q+3 of the seed
+            int q = (x >= c.param[0] ? 1 : 0) + (y >= c.param[1] ? 2 : 0);
+            r = 0.1 + 1.9 * unit_draw(c.seed, 4 * q + 0);
+            u = -1. + 2. * unit_draw(c.seed, 4 * q + 1);
+            v = -1. + 2. * unit_draw(c.seed, 4 * q + 2);
+            p = 0.1 + 1.9 * unit_draw(c.seed, 4 * q + 3);
+            break;
+        }
+        case FVB_CASE_KEEP_SOD: {
+            // keep_fv circular Sod (keep_fv_euler_2d.cu:457-463)
+            double rr = sqrt((x - 0.5) * (x - 0.5) + (y - 0.5) * (y - 0.5));
+            double phi = 0.5 * (1. + tanh((0.25 - rr) / (1.0 * h)));
+            r = 0.125 + (1.0 - 0.125) * phi;
+            p = 0.1 + (1.0 - 0.1) * phi;
+            break;
+        }
+        case FVB_CASE_LMV: {
+            // stationary low-Mach vortex (keep_fv_euler_2d.cu:472-495)
+            double eps = c.param[0], p0 = 1. / (gam * eps * eps) - 0.5;
+            double dx = x - 0.5, dy = y - 0.5, rr = sqrt(dx * dx + dy * dy);
+            double vp = (rr < 0.2) ? 5. * rr : (rr < 0.4) ? 2. - 5. * rr : 0.;
+            double ir = (rr > 1e-30) ? 1. / rr : 0.;
+            r = 1.;
+            u = -vp * dy * ir;
+            v = vp * dx * ir;
+            p = (rr < 0.2) ? p0 + 12.5 * rr * rr
+                : (rr < 0.4) ? p0 + 4. * log(5. * rr) + 4. - 20. * rr + 12.5 * rr * rr
+                             : p0 + 4. * log(2.) - 2.;
+            break;
+        }
+        default:
+            r = c.param[0]; u = c.param[1]; v = c.param[2]; p = c.param[3];
+        }
+        out[k] = r;
+        out[n2 + k] = u;
+        out[2 * n2 + k] = v;
+        out[3 * n2 + k] = p;
+    }
+}
+
+cudaError_t init_case_prim64(double *out, int n, double x0, double y0, double h, double gam,
+                             const fvb_case &c, cudaStream_t s)
+{
+    int blocks = (int)(((long long)n * n + 255) / 256);
+    if (blocks > 8192) blocks = 8192;
+    ic_kernel<<<blocks, 256, 0, s>>>(out, n, x0, y0, h, gam, c);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion
+// ---------------------------------------------------------------------------
+template <class T> __device__ __forceinline__ double ld64(const void *p, long long i)
+{
+    return (double)((const T *)p)[i];
+}
+
+__device__ __forceinline__ void prim_to_cons64(const double w[4], double c[4], double gam)
+{
+    c[0] = w[0];
+    c[1] = w[0] * w[1];
+    c[2] = w[0] * w[2];
+    c[3] = w[3] / (gam - 1.) + 0.5 * w[0] * (w[1] * w[1] + w[2] * w[2]);
+}
+__device__ __forceinline__ void cons_to_prim64(const double c[4], double w[4], double gam)
+{
+    w[0] = c[0];
+    w[1] = c[1] / c[0];
+    w[2] = c[2] / c[0];
+    w[3] = (gam - 1.) * (c[3] - 0.5 * (c[1] * c[1] + c[2] * c[2]) / c[0]);
+}
+
+// Caller array (ext: IDX_P padded or interior-only, prim or cons, f32/f64)
+// -> internal buffer(s).  Internal kinds: prim in R (F64/F32 modes) or
+// conserved hi/lo float pairs (F32C).  Only interior cells are converted;
+// the ghosts are refilled afterwards.
+__global__ void import_kernel(const void *src, ExtView e, void *dst, void *dst_lo, BufView v, int internal,
+                              double gam)
+{
+    const int n = v.n;
+    const long long n2 = (long long)n * n;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
+         k += (long long)blockDim.x * gridDim.x) {
+        const int j = (int)(k / n), i = (int)(k % n);
+        long long es = e.interior ? k : (long long)(j + e.g) * e.np + (i + e.g);
+        long long eplane = e.interior ? n2 : (long long)e.np * e.np;
+        double x[4];
+        for (int q = 0; q < 4; ++q)
+            x[q] = e.dtype == FVB_F64 ? ld64<double>(src, es + q * eplane) : ld64<float>(src, es + q * eplane);
+        long long d = (long long)(j + v.g) * v.pitch + (i + v.g) + v.xoff;
+        if (internal == INT_CONS_HILO) {
+            double c[4];
+            if (e.layout == FVB_LAYOUT_PRIM) prim_to_cons64(x, c, gam);
+            else for (int q = 0; q < 4; ++q) c[q] = x[q];
+            for (int q = 0; q < 4; ++q) {
+                float hi = (float)c[q];
+                ((float *)dst)[d + q * v.plane] = hi;
+                ((float *)dst_lo)[d + q * v.plane] = (float)(c[q] - (double)hi);
+            }
+        } else {
+            double w[4];
+            if (e.layout == FVB_LAYOUT_CONS) cons_to_prim64(x, w, gam);
+            else for (int q = 0; q < 4; ++q) w[q] = x[q];
+            for (int q = 0; q < 4; ++q) {
+                if (internal == INT_PRIM64) ((double *)dst)[d + q * v.plane] = w[q];
+                else ((float *)dst)[d + q * v.plane] = (float)w[q];
+            }
+        }
+    }
+}
+
+// internal -> caller array, interior cells (and, for a padded caller array,
+// the ghost ring too: every padded cell is copied)
+__global__ void export_kernel(const void *src, const void *src_lo, BufView v, int internal, void *dst, ExtView e,
+                              double gam)
+{
+    const int n = v.n;
+    const int span = e.interior ? n : n + 2 * v.g;
+    const int off = e.interior ? v.g : 0;          // padded coordinate of the first exported cell
+    const long long cnt = (long long)span * span;
+    const long long eplane = e.interior ? (long long)n * n : (long long)e.np * e.np;
+    const int eo = e.interior ? 0 : e.g - v.g;     // caller's padded offset of the same cell
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cnt;
+         k += (long long)blockDim.x * gridDim.x) {
+        const int jj = (int)(k / span), ii = (int)(k % span);
+        const int jp = jj + off, ip = ii + off;
+        long long s = (long long)jp * v.pitch + ip + v.xoff;
+        double x[4];
+        if (internal == INT_CONS_HILO) {
+            for (int q = 0; q < 4; ++q)
+                x[q] = (double)((const float *)src)[s + q * v.plane] + (double)((const float *)src_lo)[s + q * v.plane];
+            if (e.layout == FVB_LAYOUT_PRIM) { double w[4]; cons_to_prim64(x, w, gam); for (int q = 0; q < 4; ++q) x[q] = w[q]; }
+        } else {
+            for (int q = 0; q < 4; ++q)
+                x[q] = internal == INT_PRIM64 ? ((const double *)src)[s + q * v.plane] : (double)((const float *)src)[s + q * v.plane];
+            if (e.layout == FVB_LAYOUT_CONS) { double c[4]; prim_to_cons64(x, c, gam); for (int q = 0; q < 4; ++q) x[q] = c[q]; }
+        }
+        long long d = e.interior ? k : (long long)(jj + eo) * e.np + (ii + eo);
+        for (int q = 0; q < 4; ++q) {
+            if (e.dtype == FVB_F64) ((double *)dst)[d + q * eplane] = x[q];
+            else ((float *)dst)[d + q * eplane] = (float)x[q];
+        }
+    }
+}
+
+cudaError_t import_state(const void *src, const ExtView &e, void *dst, void *dst_lo, const BufView &v,
+                         int internal, double gam, cudaStream_t s)
+{
+    int blocks = (int)(((long long)v.n * v.n + 255) / 256);
+    if (blocks > 8192) blocks = 8192;
+    import_kernel<<<blocks, 256, 0, s>>>(src, e, dst, dst_lo, v, internal, gam);
+    return cudaGetLastError();
+}
+
+cudaError_t export_state(const void *src, const void *src_lo, const BufView &v, int internal, void *dst,
+                         const ExtView &e, double gam, cudaStream_t s)
+{
+    long long span = e.interior ? v.n : v.n + 2 * v.g;
+    int blocks = (int)((span * span + 255) / 256);
+    if (blocks > 8192) blocks = 8192;
+    export_kernel<<<blocks, 256, 0, s>>>(src, src_lo, v, internal, dst, e, gam);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// max wave speed of a state -> ctrl->lam_acc (the prologue of
+// fv_up7_ducros_2d.cu:991-993), and FP64 conserved sums
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double block_max(double x, double *sh)
+{
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = x;
+    __syncthreads();
+    double m = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sh[w]);
+    __syncthreads();
+    return m;
+}
+
+__global__ void lam_kernel(const void *st, BufView v, int internal, double gam, unsigned long long *acc)
+{
+    __shared__ double sh[32];
+    const int n = v.n;
+    const long long n2 = (long long)n * n;
+    double m = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
+         k += (long long)blockDim.x * gridDim.x) {
+        const int j = (int)(k / n), i = (int)(k % n);
+        long long s = (long long)(j + v.g) * v.pitch + (i + v.g) + v.xoff;
+        double lam;
+        if (internal == INT_PRIM64) {
+            const double *b = (const double *)st;
+            Gas<double> gs{gam, gam - 1.0};
+            lam = fabs(b[s + v.plane]) + fabs(b[s + 2 * v.plane]) + sound<double>(b[s + 3 * v.plane], b[s], gs);
+        } else if (internal == INT_PRIM32) {
+            const float *b = (const float *)st;
+            Gas<float> gs{(float)gam, (float)gam - 1.0f};
+            lam = fabsf(b[s + v.plane]) + fabsf(b[s + 2 * v.plane]) + sound<float>(b[s + 3 * v.plane], b[s], gs);
+        } else {
+            const float *b = (const float *)st;
+            Gas<float> gs{(float)gam, (float)gam - 1.0f};
+            float c[4] = {b[s], b[s + v.plane], b[s + 2 * v.plane], b[s + 3 * v.plane]}, w[4];
+            c2p<float>(c, w, gs);
+            lam = fabsf(w[1]) + fabsf(w[2]) + sound<float>(w[3], w[0], gs);
+        }
+        m = fmax(m, lam);
+    }
+    m = block_max(m, sh);
+    if (threadIdx.x == 0) atomicMax(acc, (unsigned long long)__double_as_longlong(m));
+}
+
+cudaError_t lam_into(const void *st, const BufView &v, int internal, double gam, unsigned long long *acc,
+                     cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(acc, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    int blocks = (int)(((long long)v.n * v.n + 255) / 256);
+    if (blocks > 1184) blocks = 1184;
+    lam_kernel<<<blocks, 256, 0, s>>>(st, v, internal, gam, acc);
+    return cudaGetLastError();
+}
+
+// per-block partial sums of rho, rho u, rho v, E and a non-finite count;
+// reduced on the host in block order (deterministic)
+__global__ void sums_kernel(const void *st, const void *lo, BufView v, int internal, double gam, double *part)
+{
+    __shared__ double sh[5][32];
+    const int n = v.n;
+    const long long n2 = (long long)n * n;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
+         k += (long long)blockDim.x * gridDim.x) {
+        const int j = (int)(k / n), i = (int)(k % n);
+        long long s = (long long)(j + v.g) * v.pitch + (i + v.g) + v.xoff;
+        double c[4];
+        if (internal == INT_CONS_HILO) {
+            for (int q = 0; q < 4; ++q)
+                c[q] = (double)((const float *)st)[s + q * v.plane] + (double)((const float *)lo)[s + q * v.plane];
+        } else {
+            double w[4];
+            for (int q = 0; q < 4; ++q)
+                w[q] = internal == INT_PRIM64 ? ((const double *)st)[s + q * v.plane] : (double)((const float *)st)[s + q * v.plane];
+            prim_to_cons64(w, c, gam);
+        }
+        bool fin = isfinite(c[0]) && isfinite(c[1]) && isfinite(c[2]) && isfinite(c[3]);
+        if (fin) for (int q = 0; q < 4; ++q) acc[q] += c[q];
+        else acc[4] += 1.0;
+    }
+    for (int q = 0; q < 5; ++q) {
+        double x = acc[q];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0) sh[q][threadIdx.x >> 5] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double x = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += sh[threadIdx.x][w];
+        part[blockIdx.x * 5 + threadIdx.x] = x;
+    }
+}
+
+cudaError_t sums_partials(const void *st, const void *lo, const BufView &v, int internal, double gam, double *part,
+                          int blocks, cudaStream_t s)
+{
+    sums_kernel<<<blocks, 256, 0, s>>>(st, lo, v, internal, gam, part);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// reference contract: pointwise SSP-RK3 stage (fv_up7_ducros_2d.cu:531-590)
+// and max reduction (fv_up7_ducros_2d.cu:593-612)
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void rk3_kernel(int stage, R *Uo, const R *U0, const R *Uk, const R *L, R dt, int n, int np, int g,
+                           Gas<R> gs)
+{
+    const long long n2 = (long long)n * n, np2 = (long long)np * np;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
+         k += (long long)blockDim.x * gridDim.x) {
+        const int j = (int)(k / n), i = (int)(k % n);
+        const long long c = (long long)(j + g) * np + (i + g);
+        R w0[4], c0[4], cv[4], w[4];
+        for (int q = 0; q < 4; ++q) w0[q] = U0[q * np2 + c];
+        p2c<R>(w0, c0, gs);
+        if (stage == 1) {
+            for (int q = 0; q < 4; ++q) cv[q] = c0[q] + dt * L[q * n2 + k];
+        } else {
+            R wk[4], ck[4];
+            for (int q = 0; q < 4; ++q) wk[q] = Uk[q * np2 + c];
+            p2c<R>(wk, ck, gs);
+            if (stage == 2)
+                for (int q = 0; q < 4; ++q) cv[q] = FVB_LIT(R, 0.75) * c0[q] + FVB_LIT(R, 0.25) * (ck[q] + dt * L[q * n2 + k]);
+            else
+                for (int q = 0; q < 4; ++q)
+                    cv[q] = (FVB_LIT(R, 1.) / FVB_LIT(R, 3.)) * c0[q] + (FVB_LIT(R, 2.) / FVB_LIT(R, 3.)) * (ck[q] + dt * L[q * n2 + k]);
+        }
+        c2p<R>(cv, w, gs);
+        w[0] = floor14(w[0]);
+        w[3] = floor14(w[3]);
+        for (int q = 0; q < 4; ++q) Uo[q * np2 + c] = w[q];
+    }
+}
+
+template <class R>
+cudaError_t rk3_stage_ref(int stage, R *Uo, const R *U0, const R *Uk, const R *L, R dt, int n, int np, int g,
+                          double gam, cudaStream_t s)
+{
+    int blocks = (int)(((long long)n * n + 255) / 256);
+    if (blocks > 8192) blocks = 8192;
+    Gas<R> gs{R(gam), R(gam) - R(1)};
+    rk3_kernel<R><<<blocks, 256, 0, s>>>(stage, Uo, U0, Uk, L, dt, n, np, g, gs);
+    return cudaGetLastError();
+}
+template cudaError_t rk3_stage_ref<float>(int, float *, const float *, const float *, const float *, float, int, int,
+                                          int, double, cudaStream_t);
+template cudaError_t rk3_stage_ref<double>(int, double *, const double *, const double *, const double *, double,
+                                           int, int, int, double, cudaStream_t);
+
+// max from 0 with fmax (NaN skipped); the result is atomically max-ed into
+// *out as a non-negative bit pattern, *out cleared first by the caller
+template <class R, class U>
+__global__ void max_kernel(const R *x, size_t n, U *out)
+{
+    __shared__ double sh[32];
+    double m = 0.0;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)blockDim.x * gridDim.x)
+        m = fmax(m, (double)x[k]);
+    m = block_max(m, sh);
+    if (threadIdx.x == 0) {
+        if (sizeof(R) == 8) atomicMax((unsigned long long *)out, (unsigned long long)__double_as_longlong(m));
+        else atomicMax((unsigned int *)out, (unsigned int)__float_as_int((float)m));
+    }
+}
+
+cudaError_t max_ref(const void *x, size_t n, void *out, int dtype, cudaStream_t s)
+{
+    size_t bytes = dtype == FVB_F64 ? 8 : 4;
+    cudaError_t e = cudaMemsetAsync(out, 0, bytes, s);
+    if (e != cudaSuccess) return e;
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 1184) blocks = 1184;
+    if (blocks < 1) blocks = 1;
+    if (dtype == FVB_F64) max_kernel<double, unsigned long long><<<blocks, 256, 0, s>>>((const double *)x, n, (unsigned long long *)out);
+    else max_kernel<float, unsigned int><<<blocks, 256, 0, s>>>((const float *)x, n, (unsigned int *)out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// step-control updates issued between steps
+// ---------------------------------------------------------------------------
+__global__ void ctrl_set_kernel(Ctrl *c, double t_stop, int reset, double t0, double cfl, double h)
+{
+    if (reset) {
+        c->t = t0;
+        c->dt = 0.0;
+        c->step = 0;
+        c->status = 0;
+        c->active = 0;
+        c->clamped = 0;
+        c->cfl = cfl;
+        c->h = h;
+    }
+    c->t_stop = t_stop;
+}
+
+cudaError_t ctrl_set(Ctrl *c, double t_stop, int reset, double t0, double cfl, double h, cudaStream_t s)
+{
+    ctrl_set_kernel<<<1, 1, 0, s>>>(c, t_stop, reset, t0, cfl, h);
+    return cudaGetLastError();
+}
+
+}  // namespace fvb

@@ -1,0 +1,43 @@
+// fvb_aux.h -- declarations of the kernels in fvb_aux.cu.
+#pragma once
+#include "fvb_internal.h"
+
+namespace fvb {
+
+// geometry of an internal padded buffer (see GridDev)
+struct BufView {
+    int n, g;
+    int pitch, xoff;
+    long long plane;
+};
+
+// geometry of a caller array: IDX_P padded (np = n + 2g) or interior (n x n)
+struct ExtView {
+    int interior;
+    int g, np;
+    int layout;  // fvb_layout
+    int dtype;   // fvb_dtype
+};
+
+// internal state kinds
+enum { INT_PRIM64 = 0, INT_PRIM32 = 1, INT_CONS_HILO = 2 };
+
+template <class R>
+cudaError_t bc_fill(R *buf, const BufView &v, int bcx, int bcy, cudaStream_t s);
+cudaError_t init_case_prim64(double *out, int n, double x0, double y0, double h, double gam, const fvb_case &c,
+                             cudaStream_t s);
+cudaError_t import_state(const void *src, const ExtView &e, void *dst, void *dst_lo, const BufView &v,
+                         int internal, double gam, cudaStream_t s);
+cudaError_t export_state(const void *src, const void *src_lo, const BufView &v, int internal, void *dst,
+                         const ExtView &e, double gam, cudaStream_t s);
+cudaError_t lam_into(const void *st, const BufView &v, int internal, double gam, unsigned long long *acc,
+                     cudaStream_t s);
+cudaError_t sums_partials(const void *st, const void *lo, const BufView &v, int internal, double gam,
+                          double *part, int blocks, cudaStream_t s);
+template <class R>
+cudaError_t rk3_stage_ref(int stage, R *Uo, const R *U0, const R *Uk, const R *L, R dt, int n, int np, int g,
+                          double gam, cudaStream_t s);
+cudaError_t max_ref(const void *x, size_t n, void *out, int dtype, cudaStream_t s);
+cudaError_t ctrl_set(Ctrl *c, double t_stop, int reset, double t0, double cfl, double h, cudaStream_t s);
+
+}  // namespace fvb

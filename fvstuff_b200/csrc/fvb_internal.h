@@ -1,0 +1,87 @@
+// fvb_internal.h -- device-side data structures shared by the kernels and
+// the host library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/fvb.h"
+
+namespace fvb {
+
+// Device-resident step control of one grid.  The stage kernels read and
+// update it themselves, so a run of steps needs no host round trip:
+//   stage 1 : every CTA derives dt from lam_acc (max wave speed of the
+//             current state), t and t_stop, identically; the CTA holding
+//             tile 0 ("leader") publishes dt / active
+//   stage 2 : leader clears lam_acc
+//   stage 3 : every CTA max-reduces lam of the new state into lam_acc;
+//             leader advances t and step
+// Fields a stage writes are never read by another CTA of the same stage.
+struct Ctrl {
+    double t;                   // simulated time (always FP64)
+    double t_stop;              // steps stop when t >= t_stop
+    double dt;                  // dt of the step in progress
+    double cfl, h;              // dt = cfl * h / lam
+    unsigned long long lam_acc; // bit pattern of max lam (non-negative double)
+    unsigned long long lam_cur; // lam_acc that set the current dt
+    long long step;
+    int active;                 // the step in progress runs
+    int status;                 // fvb_status of the step control
+    int clamped;                // dt was clamped to land on t_stop
+    int pad;
+};
+
+// Device view of one grid.  Element (q, jp, ip) of a padded buffer, padded
+// coordinates jp, ip in [0, n + 2g), sits at q*plane + jp*pitch + xoff + ip.
+// The IDX_P layout of the reference is pitch = n + 2g, xoff = 0,
+// plane = pitch * (n + 2g).
+struct GridDev {
+    int n, g;
+    int pitch, xoff;
+    long long plane;
+    int bcx, bcy;
+    double h, gam;
+    void *st[2];    // state: prim (F64/F32, st[0] only) or conserved hi (F32C, ping-pong)
+    void *lo[2];    // F32C: lo words of the conserved state
+    void *k1, *k2;  // stage outputs: U1/U2 primitives (F64/F32) or increments d1/d2 (F32C)
+    Ctrl *ctrl;
+    int tiles_x;    // tiles along x for the kernel's tile width
+    int pad;
+};
+
+// Tile-table entry of the batched launch: grid index and tile index.
+struct TileRef {
+    int grid;
+    int tile;
+};
+
+enum Prec { P64 = 0, P32 = 1, P32C = 2 };
+
+struct StageArgs {
+    GridDev grid;              // single-grid launches
+    const GridDev *grids;      // batched launches: grid descriptors
+    const TileRef *tiles;      // batched launches: tile table
+    const int *ntiles;         // batched launches: live tile count (device)
+    int ntiles_static;         // single-grid launches: tiles
+    int stage;                 // 1, 2, 3; 0 = residual only (reference contract)
+    int parity;                // F32C: index of the current state buffer
+    void *rhs, *lam;           // stage 0 outputs, (4, n, n) and (n, n) unpadded
+};
+
+// Tile shapes the stage kernel is instantiated for (tile width x height,
+// threads per CTA).  Chosen so the face count (TX+1)TY + TX(TY+1) is close
+// to a multiple of the thread count.
+struct TileShape {
+    int tx, ty, nt;
+};
+constexpr int kNumTileShapes = 4;
+constexpr TileShape kTileShapes[kNumTileShapes] = {
+    {32, 15, 256}, {32, 7, 128}, {64, 7, 256}, {16, 15, 256}};
+
+// launchers (fvb_stage.cu)
+cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int grid_ctas,
+                         cudaStream_t s);
+size_t stage_smem_bytes(int prec, int order, int shape);
+int stage_max_ctas_per_sm(int prec, int order, int shape);
+
+}  // namespace fvb

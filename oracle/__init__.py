@@ -1,0 +1,275 @@
+"""The oracle -- TEST INFRASTRUCTURE ONLY.
+
+ctypes access to
+  * ``liboracle.so``: the plain-C restatement of fvStuff's finite-volume step
+    (fvb_oracle.c), and
+  * ``_ref/*.so``: the reference's own kernels compiled for the host and for
+    the GPU (built by oracle/build.py from the reference checkout).
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of bench.py
+use this package, and only as the checker or the timed CPU baseline; the
+product library (fvstuff_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF = HERE / "_ref"
+
+_D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
+_libs: dict[str, C.CDLL] = {}
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_D if a.dtype == np.float64 else _F)
+
+
+def _load(path: Path) -> C.CDLL:
+    key = str(path)
+    if key not in _libs:
+        if not path.exists():
+            raise FileNotFoundError("%s is not built (run oracle/build.py)" % path)
+        _libs[key] = C.CDLL(key)
+    return _libs[key]
+
+
+def lib() -> C.CDLL:
+    p = HERE / "liboracle.so"
+    if not p.exists():
+        from . import build as _b
+        _b.build_oracle()
+    return _load(p)
+
+
+def have_ref_host() -> bool:
+    return (REF / "libref_host_up7_f64.so").exists()
+
+
+def have_ref_gpu() -> bool:
+    return (REF / "libref_gpu_up7_f64.so").exists()
+
+
+def ref_host(kind: str) -> C.CDLL:
+    """kind: 'up7_f32', 'up7_f64' or 'keep'."""
+    return _load(REF / ("libref_host_%s.so" % kind))
+
+
+def ref_gpu(kind: str) -> C.CDLL:
+    return _load(REF / ("libref_gpu_%s.so" % kind))
+
+
+def _sfx(dtype) -> str:
+    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+
+def _real(dtype):
+    return C.c_double if np.dtype(dtype) == np.float64 else C.c_float
+
+
+def ghost_width(order: int = 7) -> int:
+    return (order + 1) // 2
+
+
+def padded(N: int, g: int, dtype=np.float64) -> np.ndarray:
+    return np.zeros((4, N + 2 * g, N + 2 * g), dtype=dtype)
+
+
+# ---------------------------------------------------------------------------
+# restatement (liboracle.so)
+# ---------------------------------------------------------------------------
+def up_rhs(Q: np.ndarray, N: int, h: float, order: int = 7):
+    """Residual (4,N,N) and lam (N,N) of a padded primitive state."""
+    g = ghost_width(order)
+    assert Q.shape == (4, N + 2 * g, N + 2 * g) and Q.flags.c_contiguous
+    s = _sfx(Q.dtype)
+    R = np.empty((4, N, N), Q.dtype)
+    lam = np.empty((N, N), Q.dtype)
+    getattr(lib(), "orc_up_rhs_" + s)(_ptr(Q), _ptr(R), _ptr(lam), C.c_int(N), C.c_int(g),
+                                      C.c_int(order), _real(Q.dtype)(h))
+    return R, lam
+
+
+def bc(Q: np.ndarray, N: int, g: int, kind: int) -> None:
+    getattr(lib(), "orc_bc_" + _sfx(Q.dtype))(_ptr(Q), C.c_int(N), C.c_int(g), C.c_int(kind))
+
+
+def rk3(stage, Uo, U0, Uk, L, dt, N, g) -> None:
+    getattr(lib(), "orc_rk3_" + _sfx(Uo.dtype))(C.c_int(stage), _ptr(Uo), _ptr(U0), _ptr(Uk), _ptr(L),
+                                                _real(Uo.dtype)(dt), C.c_int(N), C.c_int(g))
+
+
+def up_run(U: np.ndarray, N: int, h: float, cfl: float, bc_kind: int, max_steps: int,
+           t_stop: float = 1e30, order: int = 7):
+    """Advance U (padded primitives, ghosts filled) in place; returns
+    (status, t, steps, lam_max, last_dt)."""
+    g = ghost_width(order)
+    info = np.zeros(4)
+    st = getattr(lib(), "orc_up_run_" + _sfx(U.dtype))(
+        _ptr(U), C.c_int(N), C.c_int(g), C.c_int(order), C.c_int(bc_kind), _real(U.dtype)(h),
+        _real(U.dtype)(cfl), C.c_int(max_steps), C.c_double(t_stop), _ptr(info))
+    return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3])
+
+
+def ic_sod(N: int, h: float, dtype=np.float64, order: int = 7) -> np.ndarray:
+    g = ghost_width(order)
+    U = padded(N, g, dtype)
+    getattr(lib(), "orc_ic_sod_" + _sfx(dtype))(_ptr(U), C.c_int(N), C.c_int(g), _real(dtype)(h))
+    return U
+
+
+def hllc(L, R, dtype=np.float64):
+    L = np.ascontiguousarray(L, dtype); R = np.ascontiguousarray(R, dtype); F = np.empty(4, dtype)
+    getattr(lib(), "orc_hllc_" + _sfx(dtype))(_ptr(L), _ptr(R), _ptr(F))
+    return F
+
+
+def hlle(L, R, dtype=np.float64):
+    L = np.ascontiguousarray(L, dtype); R = np.ascontiguousarray(R, dtype); F = np.empty(4, dtype)
+    getattr(lib(), "orc_hlle_" + _sfx(dtype))(_ptr(L), _ptr(R), _ptr(F))
+    return F
+
+
+def upface(order, s, dtype=np.float64):
+    s = np.ascontiguousarray(s, dtype)
+    vL = np.empty(1, dtype); vR = np.empty(1, dtype)
+    getattr(lib(), "orc_upface_" + _sfx(dtype))(C.c_int(order), _ptr(s), _ptr(vL), _ptr(vR))
+    return float(vL[0]), float(vR[0])
+
+
+# KEEP family ---------------------------------------------------------------
+def keep_rhs(Q: np.ndarray, N: int, h: float):
+    R = np.empty((4, N, N)); lam = np.empty((N, N)); ed = np.empty((N, N))
+    lib().orc_keep_ed(_ptr(Q), _ptr(ed), C.c_int(N))
+    edmax = float(max(0.0, np.nanmax(ed))) if ed.size else 0.0
+    lib().orc_keep_rhs(_ptr(Q), _ptr(R), _ptr(lam), C.c_int(N), C.c_double(h), C.c_double(edmax))
+    return R, lam, edmax
+
+
+def keep_run(U: np.ndarray, N: int, h: float, cfl: float, max_steps: int, t_stop: float = 1e30):
+    info = np.zeros(4)
+    st = lib().orc_keep_run(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(cfl), C.c_int(max_steps),
+                            C.c_double(t_stop), _ptr(info))
+    return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3])
+
+
+def keep_ic(N: int, h: float, lmv: bool = False, eps: float = 0.1) -> np.ndarray:
+    U = padded(N, 2)
+    if lmv:
+        lib().orc_keep_ic_lmv(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(eps))
+    else:
+        lib().orc_keep_ic_sod(_ptr(U), C.c_int(N), C.c_double(h))
+    return U
+
+
+def keep_err_lmv(U: np.ndarray, N: int, h: float, eps: float = 0.1):
+    out = np.zeros(2)
+    lib().orc_keep_err_lmv(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(eps), _ptr(out))
+    return float(out[0]), float(out[1])
+
+
+# ---------------------------------------------------------------------------
+# the reference's own kernels, host build (oracle/_ref/libref_host_*.so)
+# ---------------------------------------------------------------------------
+def ref_set_threads(n: int) -> None:
+    for k in ("up7_f32", "up7_f64", "keep"):
+        try:
+            ref_host(k).ref_set_threads(C.c_int(n))
+        except FileNotFoundError:
+            pass
+
+
+def ref_up_rhs(Q: np.ndarray, N: int, h: float):
+    s = _sfx(Q.dtype)
+    L = ref_host("up7_" + s)
+    Np = Q.shape[-1]
+    R = np.empty((4, N, N), Q.dtype); lam = np.empty((N, N), Q.dtype)
+    getattr(L, "ref_up7_rhs_" + s)(_ptr(Q), _ptr(R), _ptr(lam), C.c_int(N), C.c_int(Np), _real(Q.dtype)(h))
+    return R, lam
+
+
+def ref_up_bc(Q: np.ndarray, N: int, kind: int) -> None:
+    s = _sfx(Q.dtype)
+    getattr(ref_host("up7_" + s), "ref_up7_bc_" + s)(_ptr(Q), C.c_int(N), C.c_int(Q.shape[-1]), C.c_int(kind))
+
+
+def ref_up_ic_sod(N: int, h: float, dtype=np.float64) -> np.ndarray:
+    s = _sfx(dtype)
+    U = padded(N, 4, dtype)
+    getattr(ref_host("up7_" + s), "ref_up7_ic_sod_" + s)(_ptr(U), C.c_int(N), C.c_int(N + 8), _real(dtype)(h))
+    return U
+
+
+def ref_up_run(U: np.ndarray, N: int, h: float, cfl: float, bc_kind: int, max_steps: int,
+               t_stop: float = 1e30):
+    s = _sfx(U.dtype)
+    info = np.zeros(4)
+    st = getattr(ref_host("up7_" + s), "ref_up7_run_" + s)(
+        _ptr(U), C.c_int(N), _real(U.dtype)(h), _real(U.dtype)(cfl), C.c_int(bc_kind), C.c_int(max_steps),
+        C.c_double(t_stop), _ptr(info))
+    return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3])
+
+
+def ref_keep_rhs(Q: np.ndarray, N: int, h: float):
+    L = ref_host("keep")
+    Np = Q.shape[-1]
+    R = np.empty((4, N, N)); lam = np.empty((N, N)); ed = np.empty((N, N))
+    L.ref_keep_ed(_ptr(Q), _ptr(ed), C.c_int(N), C.c_int(Np))
+    edmax = float(max(0.0, np.nanmax(ed)))
+    L.ref_keep_rhs(_ptr(Q), _ptr(R), _ptr(lam), C.c_int(N), C.c_int(Np), C.c_double(h), C.c_double(edmax))
+    return R, lam, edmax
+
+
+def ref_keep_ic(N: int, h: float, lmv: bool = False, eps: float = 0.1) -> np.ndarray:
+    U = padded(N, 2)
+    ref_host("keep").ref_keep_ic(_ptr(U), C.c_int(N), C.c_int(N + 4), C.c_double(h), C.c_int(int(lmv)),
+                                 C.c_double(eps))
+    return U
+
+
+def ref_keep_run(U: np.ndarray, N: int, h: float, cfl: float, max_steps: int, t_stop: float = 1e30):
+    info = np.zeros(4)
+    st = ref_host("keep").ref_keep_run(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(cfl), C.c_int(max_steps),
+                                       C.c_double(t_stop), _ptr(info))
+    return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3])
+
+
+# ---------------------------------------------------------------------------
+# the reference's own kernels on the GPU (oracle/_ref/libref_gpu_*.so)
+# ---------------------------------------------------------------------------
+def refg_up_rhs(Q: np.ndarray, N: int, h: float):
+    s = _sfx(Q.dtype)
+    R = np.empty((4, N, N), Q.dtype); lam = np.empty((N, N), Q.dtype)
+    e = getattr(ref_gpu("up7_" + s), "refg_up7_rhs_" + s)(_ptr(Q), _ptr(R), _ptr(lam), C.c_int(N),
+                                                          C.c_int(Q.shape[-1]), _real(Q.dtype)(h))
+    if e:
+        raise RuntimeError("reference GPU rhs failed: cuda error %d" % e)
+    return R, lam
+
+
+def refg_up_run(U: np.ndarray, N: int, h: float, cfl: float, bc_kind: int, max_steps: int,
+                t_stop: float = 1e30):
+    """Returns (status, t, steps, lam_max, last_dt, ms of the stepping loop)."""
+    s = _sfx(U.dtype)
+    info = np.zeros(4)
+    ms = C.c_float(0)
+    st = getattr(ref_gpu("up7_" + s), "refg_up7_run_" + s)(
+        _ptr(U), C.c_int(N), _real(U.dtype)(h), _real(U.dtype)(cfl), C.c_int(bc_kind), C.c_int(max_steps),
+        C.c_double(t_stop), _ptr(info), C.byref(ms))
+    if st > 0:
+        raise RuntimeError("reference GPU run failed: cuda error %d" % st)
+    return -int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3]), float(ms.value)
+
+
+def refg_keep_run(U: np.ndarray, N: int, h: float, cfl: float, max_steps: int, t_stop: float = 1e30):
+    info = np.zeros(4)
+    ms = C.c_float(0)
+    st = ref_gpu("keep").refg_keep_run(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(cfl), C.c_int(max_steps),
+                                       C.c_double(t_stop), _ptr(info), C.byref(ms))
+    if st > 0:
+        raise RuntimeError("reference GPU run failed: cuda error %d" % st)
+    return -int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3]), float(ms.value)

@@ -1,0 +1,156 @@
+"""Build recipe for the oracle -- TEST INFRASTRUCTURE ONLY.
+
+Two things are built here, both outside the product:
+
+* ``oracle/liboracle.so`` -- the plain-C restatement (fvb_oracle.c), compiled
+  with ``-ffp-contract=off`` so each operation rounds once, as written.
+* ``oracle/_ref/`` -- the reference solvers' own kernels, compiled from the
+  files where they lie in the read-only reference checkout
+  (``FVB_REFERENCE_DIR``, default ``/root/reference``):
+
+  - host builds (g++ + OpenMP) of the device functions and grid-stride
+    kernels, taken by line range from the reference source and compiled
+    through ``ref_shim.h`` (the launches and ``main`` cannot be compiled by
+    g++, so those line ranges are left out);
+  - GPU builds (nvcc, sm_100a) that ``#include`` the whole reference file
+    with its ``main`` renamed;
+  - for ``fv_up7_ducros_2d.cu``, both as shipped (FP32) and as a mechanical
+    float->double retype (FP64), which is what the FP64 product path is
+    held to.
+
+  Everything generated goes to ``oracle/_ref/`` (git-ignored).  When the
+  reference checkout is absent the prebuilt files there are used as they are.
+"""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+REF_DIR = Path(os.environ.get("FVB_REFERENCE_DIR", "/root/reference"))
+
+UP7 = "fv_up7_ducros_2d.cu"
+KEEP = "keep_fv_euler_2d.cu"
+# line ranges g++ can compile: constants, device helpers, grid kernels, IC.
+# Left out: includes, the CK() error macro, the shared-memory reduction with
+# its <<<>>> launches, image output and main.
+UP7_HOST_LINES = [(26, 38), (48, 590), (614, 639)]
+KEEP_HOST_LINES = [(46, 68), (78, 393), (441, 536)]
+
+NVCC = os.environ.get("NVCC", "nvcc")
+GPU_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("command failed (%d): %s\n%s" % (r.returncode, " ".join(cmd), r.stdout))
+
+
+def _stale(out: Path, deps: list[Path]) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(d.exists() and d.stat().st_mtime > t for d in deps)
+
+
+def retype_f64(text: str) -> str:
+    """float -> double, single-precision math calls -> double ones, and the
+    ``f`` suffix dropped from every floating literal."""
+    text = re.sub(r"\bfloat\b", "double", text)
+    for fn in ("sqrt", "fabs", "fmin", "fmax", "tanh", "exp", "log", "pow", "sin", "cos"):
+        text = re.sub(r"\b%sf\(" % fn, fn + "(", text)
+    text = re.sub(r"(?<![\w.])((?:\d+\.\d*|\.\d+|\d+)(?:[eE][-+]?\d+)?)f\b", r"\1", text)
+    left = re.findall(r"(?<![\w.])(?:\d+\.\d*|\.\d+)(?:[eE][-+]?\d+)?f\b", text)
+    if left:
+        raise RuntimeError("retype left float literals: %r" % left[:5])
+    return text
+
+
+def _extract(src: Path, ranges: list[tuple[int, int]]) -> str:
+    lines = src.read_text().splitlines()
+    parts = []
+    for a, b in ranges:
+        parts.append("#line %d \"%s\"" % (a, src))
+        parts.extend(lines[a - 1:b])
+    return "\n".join(parts) + "\n"
+
+
+def _write_if_changed(p: Path, text: str) -> None:
+    if p.exists() and p.read_text() == text:
+        return
+    p.write_text(text)
+
+
+def build_oracle(verbose: bool = False) -> Path:
+    out = HERE / "liboracle.so"
+    deps = [HERE / "fvb_oracle.c", HERE / "fvb_oracle_up7.h", HERE / "fvb_oracle_keep.h", HERE / "build.py"]
+    if _stale(out, deps):
+        _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off",
+              "-o", str(out), str(HERE / "fvb_oracle.c"), "-lm"])
+        if verbose:
+            print("built", out)
+    return out
+
+
+def build_ref(verbose: bool = False, gpu: bool = True) -> list[Path]:
+    """Compile the reference kernels into oracle/_ref/ (host and GPU)."""
+    up7, keep = REF_DIR / UP7, REF_DIR / KEEP
+    if not (up7.exists() and keep.exists()):
+        return []
+    OUT.mkdir(exist_ok=True)
+    up7_text = up7.read_text()
+    _write_if_changed(OUT / "up7_host_f32.inc", _extract(up7, UP7_HOST_LINES))
+    _write_if_changed(OUT / "up7_host_f64.inc", retype_f64(_extract(up7, UP7_HOST_LINES)))
+    _write_if_changed(OUT / "keep_host.inc", _extract(keep, KEEP_HOST_LINES))
+    _write_if_changed(OUT / "fv_up7_f64.cu", retype_f64(up7_text))
+
+    host_flags = ["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared",
+                  "-ffp-contract=off", "-march=x86-64-v3", "-w", "-I", str(HERE)]
+    host = [
+        ("libref_host_up7_f32.so", ["-DREF_UP7", "-DREF_REAL=float", "-DREF_SFX=f32",
+                                    '-DREF_INC="_ref/up7_host_f32.inc"'], OUT / "up7_host_f32.inc"),
+        ("libref_host_up7_f64.so", ["-DREF_UP7", "-DREF_REAL=double", "-DREF_SFX=f64",
+                                    '-DREF_INC="_ref/up7_host_f64.inc"'], OUT / "up7_host_f64.inc"),
+        ("libref_host_keep.so", ["-DREF_KEEP", '-DREF_INC="_ref/keep_host.inc"'], OUT / "keep_host.inc"),
+    ]
+    built = []
+    for name, defs, inc in host:
+        out = OUT / name
+        if _stale(out, [inc, HERE / "ref_host.cpp", HERE / "ref_shim.h", HERE / "build.py"]):
+            _run(host_flags + defs + ["-o", str(out), str(HERE / "ref_host.cpp")])
+            if verbose:
+                print("built", out)
+        built.append(out)
+
+    if gpu:
+        gpu_flags = [NVCC, "-O3", "-std=c++17", *GPU_ARCH, "--expt-relaxed-constexpr",
+                     "-Xcompiler", "-fPIC", "-shared", "-w", "-I", str(REF_DIR), "-I", str(HERE)]
+        dev = [
+            ("libref_gpu_up7_f32.so", ["-DREF_UP7", "-DREF_REAL=float", "-DREF_SFX=f32",
+                                       '-DREF_CU="%s"' % up7], up7),
+            ("libref_gpu_up7_f64.so", ["-DREF_UP7", "-DREF_REAL=double", "-DREF_SFX=f64",
+                                       '-DREF_CU="_ref/fv_up7_f64.cu"'], OUT / "fv_up7_f64.cu"),
+            ("libref_gpu_keep.so", ["-DREF_KEEP", '-DREF_CU="%s"' % keep], keep),
+        ]
+        for name, defs, src in dev:
+            out = OUT / name
+            if _stale(out, [src, HERE / "ref_gpu.cu", HERE / "build.py"]):
+                _run(gpu_flags + defs + ["-o", str(out), str(HERE / "ref_gpu.cu")])
+                if verbose:
+                    print("built", out)
+            built.append(out)
+    return built
+
+
+def build(verbose: bool = False, gpu: bool = True) -> None:
+    build_oracle(verbose)
+    build_ref(verbose, gpu)
+
+
+if __name__ == "__main__":
+    build(verbose=True, gpu="--no-gpu" not in sys.argv)

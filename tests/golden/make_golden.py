@@ -1,0 +1,98 @@
+"""Generate the golden fixtures in tests/golden/ from the reference's own
+kernels, compiled for the host by oracle/build.py (oracle/_ref/).
+
+The reference has no test suite and no golden vectors of its own; these
+fixtures are outputs of its kernels (fv_up7_ducros_2d.cu as shipped and
+retyped to FP64, keep_fv_euler_2d.cu) on small seeded inputs, frozen so the
+oracle restatement stays pinned where the reference checkout is absent.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import ctypes as C
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent))
+sys.path.insert(0, str(HERE.parent))
+
+import oracle as O  # noqa: E402
+from cases import pad, vortex  # noqa: E402
+
+
+def _faces(dtype, seed=7, count=64):
+    """random face states, with supersonic and subsonic, left- and right-
+    moving contacts, through the reference's hllc_n / hlle_n with x and y
+    normals, and the UP7 face values of random stencils"""
+    rng = np.random.default_rng(seed)
+    sfx = "f64" if dtype == np.float64 else "f32"
+    L = O.ref_host("up7_" + sfx)
+    real = C.c_double if dtype == np.float64 else C.c_float
+    WL = np.empty((count, 4), dtype)
+    WR = np.empty((count, 4), dtype)
+    WL[:, 0] = rng.uniform(0.1, 3, count); WR[:, 0] = rng.uniform(0.1, 3, count)
+    WL[:, 3] = rng.uniform(0.1, 5, count); WR[:, 3] = rng.uniform(0.1, 5, count)
+    WL[:, 1:3] = rng.uniform(-3, 3, (count, 2)); WR[:, 1:3] = rng.uniform(-3, 3, (count, 2))
+    out = {"WL": WL, "WR": WR}
+    for name in ("hllc", "hlle"):
+        for tag, (nx, ny) in (("x", (1, 0)), ("y", (0, 1))):
+            F = np.empty((count, 4), dtype)
+            fn = getattr(L, "ref_up7_%s_%s" % (name, sfx))
+            for k in range(count):
+                a, b, f = WL[k].copy(), WR[k].copy(), np.empty(4, dtype)
+                fn(O._ptr(a), O._ptr(b), real(nx), real(ny), O._ptr(f))
+                F[k] = f
+            out["%s_%s" % (name, tag)] = F
+    S = rng.uniform(-2, 2, (count, 8)).astype(dtype)
+    up = np.empty((count, 2), dtype)
+    for k in range(count):
+        s = S[k].copy(); vl = np.empty(1, dtype); vr = np.empty(1, dtype)
+        getattr(L, "ref_up7_up7_" + sfx)(O._ptr(s), O._ptr(vl), O._ptr(vr))
+        up[k] = vl[0], vr[0]
+    out["stencil"] = S
+    out["up7"] = up
+    return out
+
+
+def main() -> None:
+    if not O.have_ref_host():
+        raise SystemExit("oracle/_ref is not built (python oracle/build.py)")
+    O.ref_set_threads(1)
+    N = 16
+    for dtype, sfx in ((np.float64, "f64"), (np.float32, "f32")):
+        np.savez_compressed(HERE / ("faces_%s.npz" % sfx), **_faces(dtype))
+        h = 1.0 / N
+        U = O.ref_up_ic_sod(N, h, dtype)
+        O.ref_up_bc(U, N, 0)
+        R, lam = O.ref_up_rhs(U, N, h)
+        U5 = U.copy()
+        info = O.ref_up_run(U5, N, h, 0.4, 0, 5)
+        np.savez_compressed(HERE / ("up7_sod16_%s.npz" % sfx), U0=U, rhs=R, lam=lam, U5=U5, info=np.array(info[:5]))
+    # periodic and transmissive harness compositions on a vortex / random state
+    for bc, tag in ((1, "periodic"), (2, "transmissive")):
+        n = 16
+        w = vortex(n, x0=-5, y0=-5, length=10.0)
+        U = pad(w, 4)
+        O.ref_up_bc(U, n, bc)
+        U5 = U.copy()
+        info = O.ref_up_run(U5, n, 10.0 / n, 0.5, bc, 5)
+        np.savez_compressed(HERE / ("up7_vortex16_%s_f64.npz" % tag), U0=U, U5=U5, info=np.array(info[:5]))
+    # KEEP
+    n = 16
+    for lmv, tag in ((False, "sod"), (True, "lmv")):
+        U = O.ref_keep_ic(n, 1.0 / n, lmv)
+        O.ref_host("keep").ref_keep_bc(O._ptr(U), C.c_int(n), C.c_int(n + 4))
+        R, lam, edm = O.ref_keep_rhs(U, n, 1.0 / n)
+        U5 = U.copy()
+        info = O.ref_keep_run(U5, n, 1.0 / n, 0.2, 5)
+        np.savez_compressed(HERE / ("keep_%s16.npz" % tag), U0=U, rhs=R, lam=lam, edmax=np.array(edm), U5=U5,
+                            info=np.array(info[:5]))
+    print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,60 @@
+"""The C-ABI library loads, exports exactly what include/fvb.h declares, and
+rejects bad configurations with a status (no GPU needed)."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+import fvstuff_b200 as F
+from fvstuff_b200 import _lib as L
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _declared():
+    text = (ROOT / "include" / "fvb.h").read_text()
+    return sorted(set(re.findall(r"FVB_API[^;(]*?\b(fvb_\w+)\s*\(", text)))
+
+
+def test_header_matches_bindings():
+    assert _declared() == sorted(L.declared_symbols())
+
+
+def test_library_exports_every_declared_symbol():
+    out = subprocess.run(["nm", "-D", "--defined-only", str(L.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = sorted(set(re.findall(r" T (fvb_\w+)", out)))
+    assert exported == _declared()
+    lib = F.lib()
+    for name in _declared():
+        assert getattr(lib, name) is not None
+
+
+def test_version_and_defaults():
+    assert F.lib().fvb_version().startswith(b"fvb")
+    cfg = L.Config()
+    F.lib().fvb_config_default(C.byref(cfg), 400)
+    assert (cfg.n, cfg.order, cfg.cfl, cfg.gamma, cfg.length) == (400, 7, 0.4, 1.4, 1.0)
+    c = F.case_params("vortex", -5, -5, 10)
+    assert list(c.param[:5]) == [5.0, 1.0, 1.0, 0.0, 0.0]
+
+
+@pytest.mark.parametrize("kw", [dict(order=4), dict(n=2), dict(precision="f32", order=5), dict(cfl=-1.0),
+                                dict(tile=99)])
+def test_invalid_configs_rejected(kw):
+    args = dict(n=32)
+    args.update(kw)
+    with pytest.raises(F.FvbError) as e:
+        F.Solver(**args)
+    assert e.value.status == L.ERR_INVALID
+
+
+def test_kernel_contract_validates_geometry():
+    st = F.lib().fvb_up_rhs(1, 1, 1, 16, 20, 7, 0.1, 1.4, 1, None)  # np < n + 2g
+    assert st == L.ERR_INVALID
+    st = F.lib().fvb_apply_bc(1, 16, 23, 0, 0, 0, 1, None)  # odd ghost ring
+    assert st == L.ERR_INVALID

@@ -1,0 +1,294 @@
+"""GPU parity of the plain FP64 path (and the FP32 drop-in mode) against the
+oracle and against the reference's own CUDA kernels (oracle/_ref GPU build),
+through the C ABI.
+
+Bar (the plain method): <= 1e-12 relative L-inf on the conserved variables
+(max over variables of max|a-b| / max|b|) after a fixed number of steps.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import fvstuff_b200 as F
+import oracle as O
+from cases import cons_to_prim, kh, pad, prim_to_cons, rel_linf, riemann4, sod, vortex
+
+pytestmark = pytest.mark.gpu
+TOL64 = 1e-12
+
+torch = pytest.importorskip("torch")
+
+
+def _padded(w, bc, g=4):
+    U = pad(np.ascontiguousarray(w), g)
+    O.bc(U, w.shape[-1], g, bc)
+    return U
+
+
+def _cons(U, g=4):
+    n = U.shape[-1] - 2 * g
+    return prim_to_cons(U[:, g:g + n, g:g + n].astype(np.float64))
+
+
+BCS = {"reflect": 0, "periodic": 1, "transmissive": 2}
+
+
+# --- kernel-level contract -------------------------------------------------
+
+@pytest.mark.parametrize("n", [8, 17, 40, 67])
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-13), (np.float32, 2e-5)])
+def test_up_rhs_matches_oracle(n, dtype, tol):
+    U = _padded(riemann4(n, seed=n).astype(dtype), 0)
+    h = 1.0 / n
+    Qd = torch.from_numpy(U).cuda()
+    rhs = torch.empty((4, n, n), dtype=Qd.dtype, device="cuda")
+    lam = torch.empty((n, n), dtype=Qd.dtype, device="cuda")
+    F.up_rhs(Qd, rhs, lam, n, n + 8, h)
+    torch.cuda.synchronize()
+    R, l = O.up_rhs(U, n, h)
+    assert rel_linf(rhs.cpu().numpy(), R) <= tol
+    assert rel_linf(lam.cpu().numpy()[None], l[None]) <= tol
+
+
+@pytest.mark.skipif(not O.have_ref_gpu(), reason="reference GPU build absent")
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-13), (np.float32, 2e-5)])
+def test_up_rhs_matches_reference_kernel(dtype, tol):
+    n = 96
+    U = O.ref_up_ic_sod(n, 1.0 / n, dtype)
+    O.ref_up_bc(U, n, 0)
+    Rr, lr = O.refg_up_rhs(U, n, 1.0 / n)
+    Qd = torch.from_numpy(U).cuda()
+    rhs = torch.empty((4, n, n), dtype=Qd.dtype, device="cuda")
+    lam = torch.empty((n, n), dtype=Qd.dtype, device="cuda")
+    F.up_rhs(Qd, rhs, lam, n, n + 8, 1.0 / n)
+    torch.cuda.synchronize()
+    assert rel_linf(rhs.cpu().numpy(), Rr) <= tol
+    assert rel_linf(lam.cpu().numpy()[None], lr[None]) <= tol
+
+
+@pytest.mark.parametrize("bcx,bcy", [(0, 0), (1, 1), (2, 2), (1, 0), (2, 1)])
+@pytest.mark.parametrize("n", [8, 13])
+def test_apply_bc_matches_oracle(bcx, bcy, n):
+    w = riemann4(n, seed=3)
+    U = pad(w, 4)
+    Ud = torch.from_numpy(U).cuda()
+    names = {v: k for k, v in BCS.items()}
+    F.apply_bc(Ud, n, n + 8, names[bcx], names[bcy])
+    torch.cuda.synchronize()
+    got = Ud.cpu().numpy()
+    if bcx == bcy:
+        ref = U.copy()
+        O.bc(ref, n, 4, bcx)
+        assert np.array_equal(got, ref)
+    else:
+        # per-axis rule: x-ghost columns follow bcx, y-ghost rows follow bcy
+        ref_x = U.copy(); O.bc(ref_x, n, 4, bcx)
+        ref_y = U.copy(); O.bc(ref_y, n, 4, bcy)
+        assert np.array_equal(got[:, 4:4 + n, :], ref_x[:, 4:4 + n, :])
+        assert np.array_equal(got[:, :, 4:4 + n], ref_y[:, :, 4:4 + n])
+
+
+@pytest.mark.parametrize("stage", [1, 2, 3])
+def test_rk3_stage_matches_oracle(stage):
+    n = 19
+    U0 = _padded(riemann4(n, seed=1), 1)
+    Uk = _padded(riemann4(n, seed=2), 1)
+    L = np.random.default_rng(stage).uniform(-1, 1, (4, n, n))
+    ref = U0.copy()
+    O.rk3(stage, ref, U0, Uk, L, 0.01, n, 4)
+    out = torch.from_numpy(U0.copy()).cuda()
+    F.rk3_stage(stage, out, torch.from_numpy(U0).cuda(), torch.from_numpy(Uk).cuda(), torch.from_numpy(L).cuda(),
+                0.01, n, n + 8)
+    torch.cuda.synchronize()
+    assert rel_linf(out.cpu().numpy(), ref) <= 1e-15
+
+
+def test_device_max_skips_nan():
+    x = torch.tensor([0.5, float("nan"), 3.25, 1.0], dtype=torch.float64, device="cuda")
+    out = torch.empty(1, dtype=torch.float64, device="cuda")
+    F.device_max(x, out)
+    assert out.item() == 3.25
+
+
+# --- fused step against the oracle ----------------------------------------
+
+CASES = {
+    "riemann4": lambda n: riemann4(n, seed=7 + n),
+    "vortex": lambda n: vortex(n),
+    "sod": lambda n: sod(n),
+}
+
+
+@pytest.mark.parametrize("bc", ["reflect", "periodic", "transmissive"])
+@pytest.mark.parametrize("n", [8, 9, 17, 37, 64])
+@pytest.mark.parametrize("case", ["riemann4", "vortex", "sod"])
+def test_step_f64_matches_oracle(bc, n, case):
+    w = CASES[case](n)
+    length = 10.0 if case == "vortex" else 1.0
+    U = _padded(w, BCS[bc])
+    s = F.Solver(n, bc=bc, length=length, x0=-5.0 if case == "vortex" else 0.0,
+                 y0=-5.0 if case == "vortex" else 0.0, cfl=0.45)
+    s.set_state(U)
+    steps = 12
+    s.step(steps)
+    st = s.sync()
+    got = s.get_state()
+    ref = U.copy()
+    status, t, k, lmax, dt = O.up_run(ref, n, length / n, 0.45, BCS[bc], steps)
+    assert st.status == 0 and st.steps == k == steps
+    assert abs(st.t - t) <= 1e-13 * t
+    assert rel_linf(_cons(got), _cons(ref)) <= TOL64
+    # the ghost ring is the boundary rule applied to the new interior
+    assert rel_linf(got, ref) <= TOL64
+
+
+@pytest.mark.parametrize("tile", [0, 1, 2, 3])
+def test_tile_variants_agree(tile):
+    n = 70
+    U = _padded(riemann4(n, seed=5), 1)
+    s = F.Solver(n, bc="periodic", tile=tile)
+    s.set_state(U)
+    s.step(6)
+    got = s.get_state()
+    ref = U.copy()
+    O.up_run(ref, n, 1.0 / n, 0.4, 1, 6)
+    assert rel_linf(_cons(got), _cons(ref)) <= TOL64
+
+
+@pytest.mark.skipif(not O.have_ref_gpu(), reason="reference GPU build absent")
+def test_vortex_256_matches_reference_cuda_kernels():
+    """The plain-method parity case: periodic isentropic vortex on [-5,5]^2,
+    256^2, UP7 + Ducros HLLC, SSP-RK3 at CFL 0.5, 100 steps, against the
+    reference's own kernels retyped to FP64 and run on this GPU."""
+    n, steps = 256, 100
+    U = _padded(vortex(n), 1)
+    ref = U.copy()
+    status, t, k, lmax, dt, ms = O.refg_up_run(ref, n, 10.0 / n, 0.5, 1, steps)
+    s = F.Solver(n, bc="periodic", x0=-5, y0=-5, length=10.0, cfl=0.5)
+    s.set_state(U)
+    s.step(steps)
+    st = s.sync()
+    assert st.steps == k == steps and abs(st.t - t) <= 1e-13
+    err = rel_linf(_cons(s.get_state()), _cons(ref))
+    print("vortex 256^2 x 100 steps: rel L-inf vs reference kernels = %.3e" % err)
+    assert err <= TOL64
+
+
+@pytest.mark.skipif(not O.have_ref_gpu(), reason="reference GPU build absent")
+def test_f32_mode_matches_shipped_fp32_kernels():
+    """FVB_PREC_F32 reproduces the solver as shipped (float state, double
+    reconstruction arithmetic) against its own FP32 kernels."""
+    n, steps = 64, 20
+    U = O.ref_up_ic_sod(n, 1.0 / n, np.float32)
+    O.ref_up_bc(U, n, 0)
+    ref = U.copy()
+    O.refg_up_run(ref, n, np.float32(1.0 / n), np.float32(0.4), 0, steps)
+    s = F.Solver(n, precision="f32")
+    s.set_state(U)
+    s.step(steps)
+    got = s.get_state(dtype=np.float32)
+    err = rel_linf(_cons(got.astype(np.float64)), _cons(ref.astype(np.float64)))
+    print("fp32 mode vs shipped kernels: %.3e" % err)
+    assert err <= 1e-5
+
+
+# --- step control ------------------------------------------------------------
+
+def test_advance_lands_on_t_stop_like_reference_loop():
+    n = 32
+    U = _padded(vortex(n), 1)
+    s = F.Solver(n, bc="periodic", x0=-5, y0=-5, length=10.0, cfl=0.5)
+    s.set_state(U)
+    st = s.advance(0.7)
+    ref = U.copy()
+    status, t, k, lmax, dt = O.up_run(ref, n, 10.0 / n, 0.5, 1, 10 ** 6, t_stop=0.7)
+    assert st.t == t == 0.7 and st.steps == k
+    assert rel_linf(_cons(s.get_state()), _cons(ref)) <= TOL64
+    # further steps at t >= t_stop do nothing
+    s.step(5, t_stop=0.7)
+    assert s.sync().steps == k
+
+
+def test_graph_and_direct_launches_agree_bitwise():
+    n = 48
+    U = _padded(riemann4(n, seed=9), 2)
+    a = F.Solver(n, bc="transmissive")
+    b = F.Solver(n, bc="transmissive")
+    b.set_graph(False)
+    for s in (a, b):
+        s.set_state(U)
+        s.step(7)
+    assert np.array_equal(a.get_state(), b.get_state())
+
+
+def test_blowup_reported_not_fatal():
+    n = 16
+    s = F.Solver(n, bc="periodic")
+    bad = np.full((4, n, n), np.nan)
+    s.set_state(bad, interior=True)
+    with pytest.raises(F.FvbError) as e:
+        s.advance(1.0)
+    assert e.value.status == F._lib.ERR_BLOWUP
+    # the solver stays usable
+    s.set_state(np.stack([np.ones((n, n)), np.zeros((n, n)), np.zeros((n, n)), np.ones((n, n))]), interior=True)
+    st = s.advance(0.01)
+    assert st.status == 0 and st.t == 0.01
+
+
+def test_conservation_periodic_f64():
+    n = 64
+    s = F.Solver(n, bc="periodic", x0=-5, y0=-5, length=10.0, cfl=0.5)
+    s.set_state(vortex(n), interior=True)
+    a = s.stats().sums
+    s.step(50)
+    b = s.stats().sums
+    for q in (0, 1, 2, 3):
+        assert abs(b[q] - a[q]) <= 1e-12 * max(abs(a[q]), 1.0)
+
+
+def test_state_roundtrip_layouts():
+    n = 20
+    w = riemann4(n, seed=4)
+    s = F.Solver(n, bc="reflect")
+    s.set_state(w, interior=True)
+    assert np.array_equal(s.get_state(interior=True), w)
+    c = s.get_state(layout="cons", interior=True)
+    assert rel_linf(c, prim_to_cons(w)) <= 1e-15
+    s.set_state(c, layout="cons", interior=True)
+    assert rel_linf(s.get_state(interior=True), w) <= 1e-14
+    f = s.get_state(dtype=np.float32, interior=True)
+    assert np.array_equal(f, w.astype(np.float32))
+    # device tensors in and out
+    d = torch.from_numpy(w).cuda()
+    s.set_state(d, interior=True)
+    out = torch.empty_like(d)
+    s.get_state(interior=True, out=out)
+    torch.cuda.synchronize()
+    assert torch.equal(out, d)
+
+
+@pytest.mark.parametrize("kind", ["vortex", "kh", "riemann4", "sod"])
+def test_device_initial_states(kind):
+    n = 48
+    if kind == "vortex":
+        s = F.Solver(n, bc="periodic", x0=-5, y0=-5, length=10.0)
+        s.init_case("vortex")
+        ref = vortex(n)
+    elif kind == "kh":
+        s = F.Solver(n, bc="periodic")
+        s.init_case("kh", seed=99)
+        ref = kh(n, seed=99)
+    elif kind == "riemann4":
+        s = F.Solver(n, bc="transmissive")
+        s.init_case("riemann4", seed=31)
+        ref = riemann4(n, seed=31)
+    else:
+        s = F.Solver(n)
+        s.init_case("sod")
+        ref = sod(n)
+    got = s.get_state(interior=True)
+    assert rel_linf(got, ref) <= 1e-13
+    assert s.sync().t == 0.0

@@ -1,0 +1,125 @@
+"""The oracle restatement (oracle/fvb_oracle.c) pinned to the reference.
+
+* against golden fixtures produced by the reference's own kernels
+  (tests/golden/make_golden.py): always run;
+* against the reference's kernels compiled for the host (oracle/_ref), on
+  seeded states of ragged sizes and every boundary condition: run where
+  that build exists.
+
+Both sides are compiled without FMA contraction, so the bar is bit-exact.
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+from cases import pad, riemann4, vortex
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.mark.parametrize("sfx,dtype", [("f64", np.float64), ("f32", np.float32)])
+def test_faces_golden(sfx, dtype):
+    z = np.load(GOLD / ("faces_%s.npz" % sfx))
+    for k in range(len(z["WL"])):
+        wl, wr = z["WL"][k], z["WR"][k]
+        # x-normal: (rho, u, v, p) is already (rho, un, ut, p)
+        assert np.array_equal(O.hllc(wl, wr, dtype), z["hllc_x"][k])
+        assert np.array_equal(O.hlle(wl, wr, dtype), z["hlle_x"][k])
+        # y-normal: relabel (u, v) -> (ut, un) and swap the momentum fluxes back
+        sw = [0, 2, 1, 3]
+        fy = O.hllc(wl[sw], wr[sw], dtype)[sw]
+        assert np.array_equal(fy, z["hllc_y"][k]), k
+        fy = O.hlle(wl[sw], wr[sw], dtype)[sw]
+        assert np.array_equal(fy, z["hlle_y"][k]), k
+        vl, vr = O.upface(7, z["stencil"][k], dtype)
+        assert (vl, vr) == tuple(z["up7"][k])
+
+
+@pytest.mark.parametrize("sfx,dtype", [("f64", np.float64), ("f32", np.float32)])
+def test_sod16_golden(sfx, dtype):
+    z = np.load(GOLD / ("up7_sod16_%s.npz" % sfx))
+    N, h = 16, 1.0 / 16
+    U = O.ic_sod(N, h, dtype)
+    O.bc(U, N, 4, 0)
+    assert np.array_equal(U, z["U0"])
+    R, lam = O.up_rhs(U, N, h)
+    assert np.array_equal(R, z["rhs"]) and np.array_equal(lam, z["lam"])
+    info = O.up_run(U, N, h, 0.4, 0, 5)
+    assert np.array_equal(U, z["U5"])
+    assert np.allclose(info, z["info"], rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("tag,bc", [("periodic", 1), ("transmissive", 2)])
+def test_vortex16_golden(tag, bc):
+    z = np.load(GOLD / ("up7_vortex16_%s_f64.npz" % tag))
+    U = z["U0"].copy()
+    O.up_run(U, 16, 10.0 / 16, 0.5, bc, 5)
+    assert np.array_equal(U, z["U5"])
+
+
+@pytest.mark.parametrize("tag,lmv", [("sod", False), ("lmv", True)])
+def test_keep_golden(tag, lmv):
+    z = np.load(GOLD / ("keep_%s16.npz" % tag))
+    n, h = 16, 1.0 / 16
+    U = O.keep_ic(n, h, lmv)
+    O.bc(U, n, 2, 1)
+    assert np.array_equal(U, z["U0"])
+    R, lam, edm = O.keep_rhs(U, n, h)
+    assert edm == float(z["edmax"])
+    assert np.array_equal(R, z["rhs"]) and np.array_equal(lam, z["lam"])
+    O.keep_run(U, n, h, 0.2, 5)
+    assert np.array_equal(U, z["U5"])
+
+
+needs_ref = pytest.mark.skipif(not O.have_ref_host(), reason="oracle/_ref host build absent")
+
+
+@needs_ref
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("bc", [0, 1, 2])
+@pytest.mark.parametrize("n", [8, 9, 17, 23])
+def test_oracle_matches_reference_host(dtype, bc, n):
+    w = riemann4(n, seed=100 + n + bc).astype(dtype)
+    U = pad(w, 4)
+    O.bc(U, n, 4, bc)
+    V = U.copy()
+    O.ref_up_bc(V, n, bc)
+    assert np.array_equal(U, V)
+    h = 1.0 / n
+    a = O.up_rhs(U, n, h)
+    b = O.ref_up_rhs(V, n, h)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    ia = O.up_run(U, n, h, 0.45, bc, 8)
+    ib = O.ref_up_run(V, n, h, 0.45, bc, 8)
+    assert ia == ib
+    assert np.array_equal(U, V)
+
+
+@needs_ref
+def test_oracle_matches_reference_host_t_stop():
+    # the frame-clamped dt (fv_up7_ducros_2d.cu:999-1001) lands on t_stop
+    n = 24
+    U = pad(vortex(n), 4)
+    O.bc(U, n, 4, 1)
+    V = U.copy()
+    ia = O.up_run(U, n, 10.0 / n, 0.5, 1, 1000, t_stop=0.3)
+    ib = O.ref_up_run(V, n, 10.0 / n, 0.5, 1, 1000, t_stop=0.3)
+    assert ia == ib and ia[1] == 0.3
+    assert np.array_equal(U, V)
+
+
+@needs_ref
+def test_keep_oracle_matches_reference_host():
+    n = 20
+    for lmv in (False, True):
+        U = O.keep_ic(n, 1.0 / n, lmv)
+        V = O.ref_keep_ic(n, 1.0 / n, lmv)
+        assert np.array_equal(U, V)
+        O.bc(U, n, 2, 1)
+        O.bc(V, n, 2, 1)
+        assert O.keep_run(U, n, 1.0 / n, 0.2, 6) == O.ref_keep_run(V, n, 1.0 / n, 0.2, 6)
+        assert np.array_equal(U, V)
