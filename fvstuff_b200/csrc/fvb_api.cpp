@@ -5,6 +5,7 @@
 // launches per step (or replays them as a CUDA graph) and never waits;
 // dt, the CFL reduction and the stop test all live on the device, so the
 // host synchronises only when it asks for the state or the step control.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -104,7 +105,7 @@ void case_defaults(fvb_case *c, int kind, double x0, double y0, double L)
         c->seed = 12345;
         break;
     case FVB_CASE_RIEMANN4:
-        c->param[0] = x0 + 0.5 * L; c->param[1] = y0 + 0.5 * L;
+        c->param[0] = x0 + 0.5 * L; c->param[1] = y0 + 0.5 * L; c->param[2] = 2.0;
         c->seed = 1;
         break;
     case FVB_CASE_LMV:
@@ -302,7 +303,10 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
         if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaStreamCreate"); }
         s->own_stream = true;
     }
-    size_t total = s->G.bytes + 256;
+    // buffers | step control | TMA descriptors (64-byte aligned)
+    const size_t ctrl_off = (s->G.bytes + 255) / 256 * 256;
+    const size_t tmap_off = ctrl_off + 256;
+    size_t total = tmap_off + TM_COUNT * sizeof(CUtensorMap);
     e = cudaMalloc(&s->block, total);
     if (e != cudaSuccess) {
         fvb_destroy(s);
@@ -311,8 +315,9 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     e = cudaMemsetAsync(s->block, 0, total, s->stream);
     if (e != cudaSuccess) { fvb_destroy(s); return cuda_fail(e, "cudaMemset"); }
     grid_pointers(s->gd, s->block, s->G, s->prec);
-    s->ctrl = (Ctrl *)((char *)s->block + s->G.bytes);
+    s->ctrl = (Ctrl *)((char *)s->block + ctrl_off);
     s->gd.ctrl = s->ctrl;
+    s->gd.tmap = nullptr;
     s->gd.bcx = cfg->bc_x;
     s->gd.bcy = cfg->bc_y;
     s->gd.h = cfg->length / cfg->n;
@@ -322,7 +327,21 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
 
     s->shape = cfg->tile >= 0 ? cfg->tile : autotune_shape(s->prec, s->order, cfg->n);
     tile_dims(s->shape, s->n, s->gd.tiles_x, s->tiles);
-    s->ctas = s->tiles;
+    {
+        CUtensorMap maps[TM_COUNT];
+        if (encode_tile_maps(s->gd, s->prec, s->order, s->shape, maps)) {
+            CUtensorMap *dmaps = (CUtensorMap *)((char *)s->block + tmap_off);
+            e = cudaMemcpyAsync(dmaps, maps, sizeof maps, cudaMemcpyHostToDevice, s->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+            if (e != cudaSuccess) { fvb_destroy(s); return cuda_fail(e, "tensor maps"); }
+            s->gd.tmap = dmaps;
+        }
+    }
+    {
+        int per_sm = stage_max_ctas_per_sm(s->prec, s->order, s->shape), sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device);
+        s->ctas = std::min(s->tiles, std::max(1, per_sm) * std::max(1, sms));
+    }
     s->graph_steps = s->prec == FVB_PREC_F32C ? 2 : 1;
     s->use_graph = cfg->n <= 512;
     e = ctrl_set(s->ctrl, 0.0, 1, 0.0, cfg->cfl, s->gd.h, s->stream);

@@ -129,12 +129,26 @@ __global__ void ic_kernel(double *out, int n, double x0, double y0, double h, do
             break;
         }
         case FVB_CASE_RIEMANN4: {
-            // quadrant q = (x >= xm) + 2 (y >= ym); draws 4q..4q+3 of the seed
-            int q = (x >= c.param[0] ? 1 : 0) + (y >= c.param[1] ? 2 : 0);
-            r = 0.1 + 1.9 * unit_draw(c.seed, 4 * q + 0);
-            u = -1. + 2. * unit_draw(c.seed, 4 * q + 1);
-            v = -1. + 2. * unit_draw(c.seed, 4 * q + 2);
-            p = 0.1 + 1.9 * unit_draw(c.seed, 4 * q + 3);
+            // quadrant q = (x >= xm) + 2 (y >= ym) takes draws 4q..4q+3 of the
+            // seed; the interfaces are tanh-smoothed over param[2] cells (0 =
+            // sharp), as the reference smooths its own Sod jump, because the
+            // unlimited UP7 scheme is not robust on sub-cell discontinuities
+            double wx, wy;
+            if (c.param[2] > 0) {
+                wx = 0.5 * (1. + tanh((x - c.param[0]) / (c.param[2] * h)));
+                wy = 0.5 * (1. + tanh((y - c.param[1]) / (c.param[2] * h)));
+            } else {
+                wx = x >= c.param[0] ? 1. : 0.;
+                wy = y >= c.param[1] ? 1. : 0.;
+            }
+            const double wq[4] = {(1. - wx) * (1. - wy), wx * (1. - wy), (1. - wx) * wy, wx * wy};
+            r = u = v = p = 0.;
+            for (int q = 0; q < 4; ++q) {
+                r += wq[q] * (0.1 + 1.9 * unit_draw(c.seed, 4 * q + 0));
+                u += wq[q] * (-1. + 2. * unit_draw(c.seed, 4 * q + 1));
+                v += wq[q] * (-1. + 2. * unit_draw(c.seed, 4 * q + 2));
+                p += wq[q] * (0.1 + 1.9 * unit_draw(c.seed, 4 * q + 3));
+            }
             break;
         }
         case FVB_CASE_KEEP_SOD: {

@@ -1,6 +1,7 @@
 // fvb_internal.h -- device-side data structures shared by the kernels and
 // the host library.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -45,9 +46,13 @@ struct GridDev {
     void *lo[2];    // F32C: lo words of the conserved state
     void *k1, *k2;  // stage outputs: U1/U2 primitives (F64/F32) or increments d1/d2 (F32C)
     Ctrl *ctrl;
+    const CUtensorMap *tmap;  // TMA descriptors of st[0], st[1], k1, k2 for the
+                              // kernel's halo box (device memory); null: plain loads
     int tiles_x;    // tiles along x for the kernel's tile width
     int pad;
 };
+
+enum { TM_ST0 = 0, TM_ST1 = 1, TM_K1 = 2, TM_K2 = 3, TM_COUNT = 4 };
 
 // Tile-table entry of the batched launch: grid index and tile index.
 struct TileRef {
@@ -77,6 +82,10 @@ struct TileShape {
 constexpr int kNumTileShapes = 4;
 constexpr TileShape kTileShapes[kNumTileShapes] = {
     {32, 15, 256}, {32, 7, 128}, {64, 7, 256}, {16, 15, 256}};
+
+// TMA descriptors (fvb_stage.cu): encode the four maps of a grid for a
+// tile shape into host memory; false if this grid cannot use TMA
+bool encode_tile_maps(const GridDev &gd, int prec, int order, int shape, CUtensorMap out[TM_COUNT]);
 
 // launchers (fvb_stage.cu)
 cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int grid_ctas,

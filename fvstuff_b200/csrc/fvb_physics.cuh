@@ -162,4 +162,129 @@ __device__ __forceinline__ void hlle(const R L[4], const R Rr[4], R F[4], const 
     F[3] = (SR * FL3 - SL * FR3 + SRL * (ER - EL)) / dS;
 }
 
+// ===========================================================================
+// Division-free forms for the throughput paths (FP64 plain and FP32c).  The
+// same formulas as above, with each quotient written as a product with one
+// reciprocal, the reciprocals shared where the reference divides by the same
+// quantity twice, 1/(gamma-1) precomputed, and the cell-centred sound speed
+// and energy of the HLLE states taken from per-cell values computed once.
+// Results differ from the reference's association order by a few ulp.
+// ===========================================================================
+
+// reciprocal and square root per arithmetic type: FP64 uses the correctly
+// rounded reciprocal; FP32 uses the hardware approximations (2 ulp)
+__device__ __forceinline__ double frcp(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float frcp(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double fsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float fsqrt(float x) { return x * rsqrtf(x); }  // x >= 1e-14 here
+
+template <class R> struct GasF {
+    R gam, igm1, gm1;  // gamma, 1/(gamma-1), gamma-1
+};
+
+// UP-ORDER face values with the weights pre-divided by their denominator
+template <class R, int ORDER>
+__device__ __forceinline__ void upface_fast(const R *s, R &vL, R &vR)
+{
+    if constexpr (ORDER == 3) {
+        const R k = R(1.0 / 6.0);
+        vL = (-s[0] + R(5) * s[1] + R(2) * s[2]) * k;
+        vR = (R(2) * s[1] + R(5) * s[2] - s[3]) * k;
+    } else if constexpr (ORDER == 5) {
+        const R k = R(1.0 / 60.0);
+        vL = (R(2) * s[0] - R(13) * s[1] + R(47) * s[2] + R(27) * s[3] - R(3) * s[4]) * k;
+        vR = (-R(3) * s[1] + R(27) * s[2] + R(47) * s[3] - R(13) * s[4] + R(2) * s[5]) * k;
+    } else {
+        const R k = R(1.0 / 420.0);
+        vL = (-R(3) * s[0] + R(25) * s[1] - R(101) * s[2] + R(319) * s[3] + R(214) * s[4] - R(38) * s[5]
+              + R(4) * s[6]) * k;
+        vR = (R(4) * s[1] - R(38) * s[2] + R(214) * s[3] + R(319) * s[4] - R(101) * s[5] + R(25) * s[6]
+              - R(3) * s[7]) * k;
+    }
+}
+
+// sound speed and total energy of a cell state (rho, a, b, p)
+template <class R>
+__device__ __forceinline__ void cell_ce(R r, R a, R b, R p, const GasF<R> &gs, R &c, R &E)
+{
+    R cs2 = gs.gam * p * frcp(r);
+    c = fsqrt(cs2 > FVB_LIT(R, 1e-14) ? cs2 : FVB_LIT(R, 1e-14));
+    E = p * gs.igm1 + R(0.5) * r * (a * a + b * b);
+}
+
+// Blended face flux, normal frame: (1-s) HLLC(L, R) + s HLLE(WL, WR) with
+// s the pressure-jump sensor of the two cells.  L, Rv: floored UP
+// reconstructions; WL, WR: cell states with their sound speeds cW* and
+// energies EW*.                               fv_up7_ducros_2d.cu:237-328, :433
+template <class R>
+__device__ __forceinline__ void face_flux_fast(const R L[4], const R Rv[4], const R WL[4], const R WR[4], R cWL,
+                                               R cWR, R EWL, R EWR, const GasF<R> &gs, R F[4])
+{
+    const R zero = R(0);
+    // --- HLLC of the reconstructed states ---
+    R Fh0, Fh1, Fh2, Fh3;
+    {
+        const R rL = L[0], uL = L[1], tL = L[2], pL = L[3];
+        const R rR = Rv[0], uR = Rv[1], tR = Rv[2], pR = Rv[3];
+        const R irL = frcp(rL), irR = frcp(rR);
+        R cs2L = gs.gam * pL * irL, cs2R = gs.gam * pR * irR;
+        const R cL = fsqrt(cs2L > FVB_LIT(R, 1e-14) ? cs2L : FVB_LIT(R, 1e-14));
+        const R cR = fsqrt(cs2R > FVB_LIT(R, 1e-14) ? cs2R : FVB_LIT(R, 1e-14));
+        const R EL = pL * gs.igm1 + R(0.5) * rL * (uL * uL + tL * tL);
+        const R ER = pR * gs.igm1 + R(0.5) * rR * (uR * uR + tR * tR);
+        const R SL = dmin<R>(uL - cL, uR - cR), SR = dmax<R>(uL + cL, uR + cR);
+        if (SL >= zero) {
+            const R m = rL * uL;
+            Fh0 = m; Fh1 = m * uL + pL; Fh2 = m * tL; Fh3 = (EL + pL) * uL;
+        } else if (SR <= zero) {
+            const R m = rR * uR;
+            Fh0 = m; Fh1 = m * uR + pR; Fh2 = m * tR; Fh3 = (ER + pR) * uR;
+        } else {
+            const R dL = rL * (SL - uL), dR = rR * (SR - uR);
+            const R Ss = (pR - pL + dL * uL - dR * uR) * frcp(dL - dR);
+            const bool left = (Ss >= zero);
+            const R rK = left ? rL : rR, uK = left ? uL : uR, tK = left ? tL : tR;
+            const R pK = left ? pL : pR, EK = left ? EL : ER, SK = left ? SL : SR;
+            const R dK = left ? dL : dR, irK = left ? irL : irR;
+            const R fact = dK * frcp(SK - Ss);
+            const R m = rK * uK;
+            Fh0 = m + SK * (fact - rK);
+            Fh1 = m * uK + pK + SK * (fact * Ss - m);
+            Fh2 = m * tK + SK * (fact * tK - rK * tK);
+            Fh3 = (EK + pK) * uK + SK * (fact * (EK * irK + (Ss - uK) * (Ss + pK * frcp(dK))) - EK);
+        }
+    }
+    // --- HLLE of the cell states ---
+    R Fl0, Fl1, Fl2, Fl3;
+    {
+        const R rL = WL[0], uL = WL[1], tL = WL[2], pL = WL[3];
+        const R rR = WR[0], uR = WR[1], tR = WR[2], pR = WR[3];
+        const R SL = dmin<R>(uL - cWL, uR - cWR), SR = dmax<R>(uL + cWL, uR + cWR);
+        const R mL = rL * uL, mR = rR * uR;
+        const R FL1 = mL * uL + pL, FR1 = mR * uR + pR;
+        const R FL3 = (EWL + pL) * uL, FR3 = (EWR + pR) * uR;
+        if (SL >= zero) {
+            Fl0 = mL; Fl1 = FL1; Fl2 = mL * tL; Fl3 = FL3;
+        } else if (SR <= zero) {
+            Fl0 = mR; Fl1 = FR1; Fl2 = mR * tR; Fl3 = FR3;
+        } else {
+            const R idS = frcp(dmax<R>(SR - SL, FVB_LIT(R, 1e-10)));
+            const R SRL = SR * SL;
+            Fl0 = (SR * mL - SL * mR + SRL * (rR - rL)) * idS;
+            Fl1 = (SR * FL1 - SL * FR1 + SRL * (mR - mL)) * idS;
+            Fl2 = (SR * mL * tL - SL * mR * tR + SRL * (rR * tR - rL * tL)) * idS;
+            Fl3 = (SR * FL3 - SL * FR3 + SRL * (EWR - EWL)) * idS;
+        }
+    }
+    // --- Ducros blend ---
+    const R dp = WR[3] - WL[3], ps = WR[3] + WL[3];
+    const R dp2 = dp * dp;
+    const R sd = dp2 * frcp(dp2 + FVB_LIT(R, 0.1) * ps * ps);
+    const R om = R(1) - sd;
+    F[0] = om * Fh0 + sd * Fl0;
+    F[1] = om * Fh1 + sd * Fl1;
+    F[2] = om * Fh2 + sd * Fl2;
+    F[3] = om * Fh3 + sd * Fl3;
+}
+
 }  // namespace fvb

@@ -15,6 +15,8 @@
 // This replaces compute_rhs + rk3_sX + apply_bc (+ reduce_max after stage 3)
 // of fv_up7_ducros_2d.cu:370-612, three launches per stage and a host sync
 // per step, by one launch per stage and none.
+#include <stdint.h>
+
 #include "fvb_internal.h"
 #include "fvb_physics.cuh"
 
@@ -87,6 +89,13 @@ __device__ __forceinline__ void df_add(float &hi, float &lo, float d)
     float h2 = __fadd_rn(s, l);
     lo = __fsub_rn(l, __fsub_rn(h2, s));
     hi = h2;
+}
+
+// does any grid of this launch load through TMA (a single-grid launch
+// decides by its descriptor; batched grids all carry descriptors)
+__device__ __forceinline__ bool gd_has_tma(const StageArgs &a)
+{
+    return a.grids != nullptr || a.grid.tmap != nullptr;
 }
 
 struct TileCtl {
@@ -172,45 +181,191 @@ __device__ __forceinline__ void leader_finish(Ctrl *c)
     c->step = c->step + 1;
 }
 
+// ---------------------------------------------------------------------------
+// TMA and mbarrier primitives (sm_90+ PTX; no cluster multicast anywhere)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// one 3-D tiled tensor load global -> shared, completing on `bar`
+__device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// bounded wait for phase `parity` of `bar`; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    for (uint32_t it = 0; it < (1u << 24); ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// The halo box of a tile in one grid: TMA when the grid has descriptors,
+// else cooperative loads by the whole CTA (the caller's IDX_P arrays).
+template <int PREC, int G, int SW, int SH, int NT, class R>
+__device__ __forceinline__ void issue_tile_load(const GridDev &gd, int stage, int parity, int tile, R *IN,
+                                                uint64_t *bar, int tid)
+{
+    constexpr int TXd = SW - 2 * G, TYd = SH - 2 * G;
+    const int tx0 = (tile % gd.tiles_x) * TXd, ty0 = (tile / gd.tiles_x) * TYd;
+    const bool two = (PREC == P32C) && (stage == 2 || stage == 3);
+    if (gd.tmap) {
+        if (tid == 0) {
+            constexpr uint32_t box = 4u * SW * SH * sizeof(R);
+            mbar_expect_tx(bar, two ? 2 * box : box);
+            int m0;
+            if (PREC == P32C) m0 = parity ? TM_ST1 : TM_ST0;
+            else m0 = stage == 2 ? TM_K1 : stage == 3 ? TM_K2 : TM_ST0;
+            const int x = gd.xoff + tx0;
+            tma_load3(IN, gd.tmap + m0, x, ty0, 0, bar);
+            if (two) tma_load3(IN + 4 * SW * SH, gd.tmap + (stage == 2 ? TM_K1 : TM_K2), x, ty0, 0, bar);
+        }
+        return;
+    }
+    const R *src = (const R *)(PREC == P32C ? gd.st[parity]
+                                            : (stage == 2 ? gd.k1 : stage == 3 ? gd.k2 : gd.st[0]));
+    const R *inc = two ? (const R *)(stage == 2 ? gd.k1 : gd.k2) : nullptr;
+    const int np = gd.n + 2 * G;
+    for (int k = tid; k < SH * SW; k += NT) {
+        int r = k / SW, c = k - r * SW;
+        int jp = ty0 + r, ip = tx0 + c;
+        bool in = jp < np && ip < np;
+        long long e = (long long)jp * gd.pitch + ip + gd.xoff;
+        for (int q = 0; q < 4; ++q) {
+            IN[q * SH * SW + k] = in ? src[e + q * gd.plane] : R(0);
+            if (two) IN[(4 + q) * SH * SW + k] = in ? inc[e + q * gd.plane] : R(0);
+        }
+    }
+}
+
 template <int PREC, int ORDER, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, 1) stage_kernel(const StageArgs a)
+__global__ void __launch_bounds__(NT, 1) stage_kernel(const __grid_constant__ StageArgs a)
 {
     using R = typename PrecT<PREC>::R;
     using RR = typename PrecT<PREC>::RR;
     constexpr int G = (ORDER + 1) / 2;
-    constexpr int SW = TX + 2 * G, SH = TY + 2 * G;
+    constexpr int SW = TX + 2 * G, SH = TY + 2 * G, PL = SW * SH;
     constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1);
     constexpr int NW = NT / 32;
+    // the throughput paths keep each cell's sound speed and energy too
+    constexpr bool FAST = (PREC != P32);
+    constexpr int NIN = PREC == P32C ? 8 : 4;  // planes of one halo box load
 
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R *S = reinterpret_cast<R *>(smem_raw);  // [4][SH][SW] primitives
-    R *FX = S + 4 * SH * SW;                 // [4][TY][TX+1]
-    R *FY = FX + 4 * TY * (TX + 1);          // [4][TY+1][TX]
+    // IN: the tile as loaded (TMA lands here); W: primitives (+ c, E) the
+    // faces are computed from, so IN can take the next tile meanwhile
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    R *IN = reinterpret_cast<R *>(smem_raw);
+    R *W = IN + NIN * PL;
+    R *FX = W + 6 * PL;               // [4][TY][TX+1]
+    R *FY = FX + 4 * TY * (TX + 1);   // [4][TY+1][TX]
     __shared__ TileCtl s_ctl;
     __shared__ double s_red[NW];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ int s_err;
 
     const int tid = threadIdx.x;
     const bool batched = (a.grids != nullptr);
     const int ntiles = batched ? *a.ntiles : a.ntiles_static;
+    const int cur = a.parity, nxt = a.parity ^ 1;
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        s_err = 0;
+    }
+    __syncthreads();
 
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        GridDev gd;
-        int tile;
+    auto grid_of = [&](int t, int &tile) -> GridDev {
         if (batched) {
             TileRef tr = a.tiles[t];
-            gd = a.grids[tr.grid];
             tile = tr.tile;
-        } else {
-            gd = a.grid;
-            tile = t;
+            return a.grids[tr.grid];
         }
+        tile = t;
+        return a.grid;
+    };
+
+    uint32_t phase = 0;
+    int t = blockIdx.x;
+    if (t < ntiles) {
+        int tile;
+        GridDev g0 = grid_of(t, tile);
+        issue_tile_load<PREC, G, SW, SH, NT>(g0, a.stage, cur, tile, IN, &s_bar, tid);
+    }
+    for (; t < ntiles; t += gridDim.x) {
+        int tile;
+        const GridDev gd = grid_of(t, tile);
         const int n = gd.n;
         const int tx0 = (tile % gd.tiles_x) * TX, ty0 = (tile / gd.tiles_x) * TY;
         if (tid == 0) s_ctl = tile_control<PREC>(gd.ctrl, a.stage, tile == 0);
+        // ---- 1. wait for this tile's halo box; convert into W --------------
+        if (gd.tmap) {
+            if (mbar_wait(&s_bar, phase)) phase ^= 1;
+            else s_err = 1;
+        }
         __syncthreads();
         const TileCtl ctl = s_ctl;
         const Gas<R> gs{R(gd.gam), R(gd.gam) - R(1)};
-        const int cur = a.parity, nxt = a.parity ^ 1;
+        const GasF<R> gf{R(gd.gam), R(1.0 / (gd.gam - 1.0)), R(gd.gam) - R(1)};
+        if (s_err) {
+            // a halo load never arrived: record it, skip the tile
+            if (tid == 0 && gd.ctrl) gd.ctrl->status = FVB_ERR_TIMEOUT;
+            break;
+        }
+        if (ctl.run && a.stage >= 0) {
+            for (int k = tid; k < PL; k += NT) {
+                R w0 = IN[k], w1 = IN[PL + k], w2 = IN[2 * PL + k], w3 = IN[3 * PL + k];
+                if constexpr (PREC == P32C) {
+                    if (a.stage >= 2) {
+                        w0 += IN[4 * PL + k]; w1 += IN[5 * PL + k]; w2 += IN[6 * PL + k]; w3 += IN[7 * PL + k];
+                    }
+                    const float ir = frcp(w0);
+                    const float E = w3;
+                    w1 *= ir;
+                    w2 *= ir;
+                    w3 = gf.gm1 * (E - 0.5f * w0 * (w1 * w1 + w2 * w2));
+                    W[5 * PL + k] = E;
+                }
+                W[k] = w0; W[PL + k] = w1; W[2 * PL + k] = w2; W[3 * PL + k] = w3;
+            }
+        }
+        __syncthreads();
+        // ---- 2. load the next tile into IN (asynchronous through TMA) -------
+        {
+            const int tn = t + gridDim.x;
+            if (tn < ntiles) {
+                int tilen;
+                const GridDev gn = grid_of(tn, tilen);
+                // order this CTA's reads of IN before the async-proxy writes
+                if (tid == 0 && gn.tmap) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                issue_tile_load<PREC, G, SW, SH, NT>(gn, a.stage, cur, tilen, IN, &s_bar, tid);
+            }
+        }
 
         if (!ctl.run) {
             if constexpr (PREC == P32C) if (ctl.copy) {
@@ -229,43 +384,27 @@ __global__ void __launch_bounds__(NT, 1) stage_kernel(const StageArgs a)
             __syncthreads();
             continue;
         }
+        // sound speed and energy of the cells the HLLE uses: the cross of
+        // the interior rows x [G-1, G+TX] and the interior columns x {G-1, G+TY}
+        if constexpr (FAST) {
+            constexpr int NA = TY * (TX + 2), NB = 2 * TX;
+            for (int k = tid; k < NA + NB; k += NT) {
+                int r, c;
+                if (k < NA) { r = G + k / (TX + 2); c = G - 1 + k % (TX + 2); }
+                else { int m = k - NA; r = (m < TX) ? G - 1 : G + TY; c = G + (m % TX); }
+                const int e = r * SW + c;
+                const R rho = W[e], u = W[PL + e], v = W[2 * PL + e], p = W[3 * PL + e];
+                const R ir = frcp(rho);
+                R cs2 = gf.gam * p * ir;
+                W[4 * PL + e] = fsqrt(cs2 > FVB_LIT(R, 1e-14) ? cs2 : FVB_LIT(R, 1e-14));
+                if constexpr (PREC != P32C) W[5 * PL + e] = p * gf.igm1 + R(0.5) * rho * (u * u + v * v);
+            }
+            __syncthreads();
+        }
         const R dt = R(ctl.dt);
         const R inv_h = R(1.0 / gd.h);
 
-        // ---- 1. halo tile -> shared memory (primitives) ----------------
-        {
-            const int np = n + 2 * G;
-            const R *src;
-            const float *inc = nullptr;
-            if constexpr (PREC == P32C) {
-                src = (const R *)gd.st[cur];
-                if (a.stage == 2) inc = (const float *)gd.k1;
-                else if (a.stage == 3) inc = (const float *)gd.k2;
-            } else {
-                src = (const R *)(a.stage == 2 ? gd.k1 : a.stage == 3 ? gd.k2 : gd.st[0]);
-            }
-            for (int k = tid; k < SH * SW; k += NT) {
-                int r = k / SW, c = k - r * SW;
-                int jp = ty0 + r, ip = tx0 + c;  // padded coordinates
-                R w[4] = {R(0), R(0), R(0), R(0)};
-                if (jp < np && ip < np) {
-                    long long e = (long long)jp * gd.pitch + ip + gd.xoff;
-                    if constexpr (PREC == P32C) {
-                        float u[4];
-                        for (int q = 0; q < 4; ++q) u[q] = __ldg(src + e + q * gd.plane);
-                        if (inc)
-                            for (int q = 0; q < 4; ++q) u[q] += __ldg(inc + e + q * gd.plane);
-                        c2p<float>(u, w, gs);
-                    } else {
-                        for (int q = 0; q < 4; ++q) w[q] = __ldg(src + e + q * gd.plane);
-                    }
-                }
-                for (int q = 0; q < 4; ++q) S[q * SH * SW + k] = w[q];
-            }
-        }
-        __syncthreads();
-
-        // ---- 2. face fluxes -------------------------------------------
+        // ---- 3. face fluxes -------------------------------------------------
         for (int f = tid; f < NXF + NYF; f += NT) {
             const bool xf = f < NXF;
             int r, c, st;
@@ -277,24 +416,30 @@ __global__ void __launch_bounds__(NT, 1) stage_kernel(const StageArgs a)
             R L[4], Rv[4], WL[4], WR[4];
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
-                const R *v = S + qs[m] * SH * SW + base;
+                const R *v = W + qs[m] * PL + base;
                 R s[2 * G];
 #pragma unroll
                 for (int d = 0; d < 2 * G; ++d) s[d] = v[(d - G) * st];
-                upface<R, RR, ORDER>(s, L[m], Rv[m]);
+                if constexpr (FAST) upface_fast<R, ORDER>(s, L[m], Rv[m]);
+                else upface<R, RR, ORDER>(s, L[m], Rv[m]);
                 WL[m] = s[G - 1];
                 WR[m] = s[G];
             }
             L[0] = floor14(L[0]); Rv[0] = floor14(Rv[0]);
             L[3] = floor14(L[3]); Rv[3] = floor14(Rv[3]);
-            R Fh[4], Fl[4];
-            hllc<R>(L, Rv, Fh, gs);
-            hlle<R>(WL, WR, Fl, gs);
-            const R sd = ducros<R>(WL[3], WR[3]);
-            const R one_m = R(1) - sd;
             R Fn[4];
+            if constexpr (FAST) {
+                const R *CE = W + 4 * PL + base;
+                face_flux_fast<R>(L, Rv, WL, WR, CE[-st], CE[0], CE[PL - st], CE[PL], gf, Fn);
+            } else {
+                R Fh[4], Fl[4];
+                hllc<R>(L, Rv, Fh, gs);
+                hlle<R>(WL, WR, Fl, gs);
+                const R sd = ducros<R>(WL[3], WR[3]);
+                const R one_m = R(1) - sd;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) Fn[q] = one_m * Fh[q] + sd * Fl[q];
+                for (int q = 0; q < 4; ++q) Fn[q] = one_m * Fh[q] + sd * Fl[q];
+            }
             if (xf) {
                 R *o = FX + r * (TX + 1) + c;
                 o[0] = Fn[0]; o[TY * (TX + 1)] = Fn[1]; o[2 * TY * (TX + 1)] = Fn[2]; o[3 * TY * (TX + 1)] = Fn[3];
@@ -305,7 +450,7 @@ __global__ void __launch_bounds__(NT, 1) stage_kernel(const StageArgs a)
         }
         __syncthreads();
 
-        // ---- 3. divergence, RK combination, stores ----------------------
+        // ---- 4. divergence, RK combination, stores ------------------------
         double lmax = 0.0;
         for (int k = tid; k < TX * TY; k += NT) {
             int r = k / TX, c = k - r * TX, i = tx0 + c, j = ty0 + r;
@@ -322,8 +467,7 @@ __global__ void __launch_bounds__(NT, 1) stage_kernel(const StageArgs a)
                 R *rhs = (R *)a.rhs;
                 size_t n2 = (size_t)n * n, kk = (size_t)j * n + i;
                 for (int q = 0; q < 4; ++q) rhs[q * n2 + kk] = res[q];
-                R lam = dabs<R>(S[SH * SW + sc]) + dabs<R>(S[2 * SH * SW + sc]) + sound<R>(S[3 * SH * SW + sc], S[sc], gs);
-                ((R *)a.lam)[kk] = lam;
+                ((R *)a.lam)[kk] = dabs<R>(W[PL + sc]) + dabs<R>(W[2 * PL + sc]) + sound<R>(W[3 * PL + sc], W[sc], gs);
                 continue;
             }
             if constexpr (PREC == P32C) {
@@ -349,7 +493,11 @@ __global__ void __launch_bounds__(NT, 1) stage_kernel(const StageArgs a)
                     }
                     // floors rho, p >= 1e-14 on the new state
                     float w[4];
-                    c2p<float>(vh, w, gs);
+                    {
+                        const float ir = frcp(vh[0]);
+                        w[0] = vh[0]; w[1] = vh[1] * ir; w[2] = vh[2] * ir;
+                        w[3] = gf.gm1 * (vh[3] - 0.5f * (vh[1] * vh[1] + vh[2] * vh[2]) * ir);
+                    }
                     if (!(w[0] > 1e-14f)) { vh[0] = 1e-14f; vl[0] = 0.f; w[0] = 1e-14f; }
                     if (!(w[3] > 1e-14f)) {
                         float ke = 0.5f * (vh[1] * vh[1] + vh[2] * vh[2]) / vh[0];
@@ -357,54 +505,78 @@ __global__ void __launch_bounds__(NT, 1) stage_kernel(const StageArgs a)
                     }
                     put_cell<float>(gd, (float *)gd.st[nxt], j, i, vh);
                     put_cell<float>(gd, (float *)gd.lo[nxt], j, i, vl);
-                    float lam = fabsf(vh[1] / vh[0]) + fabsf(vh[2] / vh[0]) + sound<float>(w[3], w[0], gs);
+                    float cs2 = gf.gam * w[3] * frcp(w[0]);
+                    float lam = fabsf(w[1]) + fabsf(w[2]) + fsqrt(cs2 > 1e-14f ? cs2 : 1e-14f);
                     lmax = fmax(lmax, (double)lam);
                 }
-                continue;
             } else {
-            // primitive-state modes (F64 / F32): the reference's update
-            R wk[4], w0[4], c0[4], cv[4], w[4];
+                // primitive-state modes (F64 / F32): the reference's update
+                R wk[4], w0[4], c0[4], cv[4], w[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) wk[q] = S[q * SH * SW + sc];
-            if (a.stage == 1) {
+                for (int q = 0; q < 4; ++q) wk[q] = W[q * PL + sc];
+                if (a.stage == 1) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) w0[q] = wk[q];
-            } else {
-                const R *u0 = (const R *)gd.st[0];
-                const long long e = gidx(gd, 0, j, i);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) w0[q] = u0[e + q * gd.plane];
-            }
-            p2c<R>(w0, c0, gs);
-            if (a.stage == 1) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) cv[q] = c0[q] + dt * res[q];
-            } else {
-                R ck[4];
-                p2c<R>(wk, ck, gs);
-                if (a.stage == 2) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        cv[q] = FVB_LIT(R, 0.75) * c0[q] + FVB_LIT(R, 0.25) * (ck[q] + dt * res[q]);
+                    for (int q = 0; q < 4; ++q) w0[q] = wk[q];
                 } else {
-                    const R a3 = FVB_LIT(R, 1.) / FVB_LIT(R, 3.), b3 = FVB_LIT(R, 2.) / FVB_LIT(R, 3.);
+                    const R *u0 = (const R *)gd.st[0];
+                    const long long e = gidx(gd, 0, j, i);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) cv[q] = a3 * c0[q] + b3 * (ck[q] + dt * res[q]);
+                    for (int q = 0; q < 4; ++q) w0[q] = u0[e + q * gd.plane];
                 }
-            }
-            c2p<R>(cv, w, gs);
-            w[0] = floor14(w[0]);
-            w[3] = floor14(w[3]);
-            R *out = (R *)(a.stage == 1 ? gd.k1 : a.stage == 2 ? gd.k2 : gd.st[0]);
-            put_cell<R>(gd, out, j, i, w);
-            if (a.stage == 3) {
-                R lam = dabs<R>(w[1]) + dabs<R>(w[2]) + sound<R>(w[3], w[0], gs);
-                lmax = fmax(lmax, (double)lam);
-            }
+                if constexpr (FAST) {
+                    c0[0] = w0[0]; c0[1] = w0[0] * w0[1]; c0[2] = w0[0] * w0[2];
+                    c0[3] = w0[3] * gf.igm1 + R(0.5) * w0[0] * (w0[1] * w0[1] + w0[2] * w0[2]);
+                } else {
+                    p2c<R>(w0, c0, gs);
+                }
+                if (a.stage == 1) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) cv[q] = c0[q] + dt * res[q];
+                } else {
+                    R ck[4];
+                    if constexpr (FAST) {
+                        ck[0] = wk[0]; ck[1] = wk[0] * wk[1]; ck[2] = wk[0] * wk[2];
+                        ck[3] = wk[3] * gf.igm1 + R(0.5) * wk[0] * (wk[1] * wk[1] + wk[2] * wk[2]);
+                    } else {
+                        p2c<R>(wk, ck, gs);
+                    }
+                    if (a.stage == 2) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            cv[q] = FVB_LIT(R, 0.75) * c0[q] + FVB_LIT(R, 0.25) * (ck[q] + dt * res[q]);
+                    } else {
+                        const R a3 = FVB_LIT(R, 1.) / FVB_LIT(R, 3.), b3 = FVB_LIT(R, 2.) / FVB_LIT(R, 3.);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) cv[q] = a3 * c0[q] + b3 * (ck[q] + dt * res[q]);
+                    }
+                }
+                if constexpr (FAST) {
+                    const R ir = frcp(cv[0]);
+                    w[0] = cv[0];
+                    w[1] = cv[1] * ir;
+                    w[2] = cv[2] * ir;
+                    w[3] = gf.gm1 * (cv[3] - R(0.5) * (cv[1] * cv[1] + cv[2] * cv[2]) * ir);
+                } else {
+                    c2p<R>(cv, w, gs);
+                }
+                w[0] = floor14(w[0]);
+                w[3] = floor14(w[3]);
+                R *out = (R *)(a.stage == 1 ? gd.k1 : a.stage == 2 ? gd.k2 : gd.st[0]);
+                put_cell<R>(gd, out, j, i, w);
+                if (a.stage == 3) {
+                    R lam;
+                    if constexpr (FAST) {
+                        R cs2 = gf.gam * w[3] * frcp(w[0]);
+                        lam = dabs<R>(w[1]) + dabs<R>(w[2]) + fsqrt(cs2 > FVB_LIT(R, 1e-14) ? cs2 : FVB_LIT(R, 1e-14));
+                    } else {
+                        lam = dabs<R>(w[1]) + dabs<R>(w[2]) + sound<R>(w[3], w[0], gs);
+                    }
+                    lmax = fmax(lmax, (double)lam);
+                }
             }
         }
 
-        // ---- 4. max wave speed of the new state (stage 3) ----------------
+        // ---- 5. max wave speed of the new state (stage 3) ------------------
         if (a.stage == 3) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
@@ -419,6 +591,9 @@ __global__ void __launch_bounds__(NT, 1) stage_kernel(const StageArgs a)
         }
         __syncthreads();
     }
+    // a load still in flight after an error: wait for it (bounded) so no
+    // copy into this CTA's shared memory outlives it
+    if (s_err && gd_has_tma(a)) mbar_wait(&s_bar, phase);
 }
 
 // ---------------------------------------------------------------------------
@@ -431,7 +606,9 @@ struct K {
     using R = typename PrecT<PREC>::R;
     static size_t smem()
     {
-        return sizeof(R) * (4 * (ts.ty + 2 * G) * (ts.tx + 2 * G) + 4 * ts.ty * (ts.tx + 1) + 4 * (ts.ty + 1) * ts.tx);
+        const int nin = PREC == P32C ? 8 : 4;
+        return sizeof(R) * ((nin + 6) * (ts.ty + 2 * G) * (ts.tx + 2 * G) + 4 * ts.ty * (ts.tx + 1) +
+                            4 * (ts.ty + 1) * ts.tx);
     }
     static void *fn() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt>; }
 };
@@ -476,6 +653,57 @@ static cudaError_t prepare(KernelEntry &e)
     e.max_ctas = nb;
     e.ready = 1;
     return cudaSuccess;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// Descriptors of the (TX+2g) x (TY+2g) x 4 halo box of each padded buffer.
+// The tensor is (x = memory column, y = padded row, z = variable plane);
+// x starts at column 0 of the pitched row, so a tile's box starts at
+// x = xoff + tx0.  Every such x, the pitch and the plane stride must be
+// 16-byte multiples; out-of-range parts of ragged tiles are zero-filled.
+bool encode_tile_maps(const GridDev &gd, int prec, int order, int shape, CUtensorMap out[TM_COUNT])
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc || shape < 0 || shape >= kNumTileShapes) return false;
+    const TileShape &ts = kTileShapes[shape];
+    const int g = (order + 1) / 2, np = gd.n + 2 * g;
+    const size_t es = prec == P64 ? 8 : 4;
+    const int sw = ts.tx + 2 * g, sh = ts.ty + 2 * g;
+    if (((size_t)gd.pitch * es) % 16 || ((size_t)gd.plane * es) % 16 || ((size_t)gd.xoff * es) % 16 ||
+        ((size_t)ts.tx * es) % 16 || ((size_t)sw * es) % 16 || sw > 256 || sh > 256)
+        return false;
+    cuuint64_t dims[3] = {(cuuint64_t)(gd.xoff + np), (cuuint64_t)np, 4};
+    cuuint64_t strides[2] = {(cuuint64_t)gd.pitch * es, (cuuint64_t)gd.plane * es};
+    cuuint32_t box[3] = {(cuuint32_t)sw, (cuuint32_t)sh, 4};
+    cuuint32_t estr[3] = {1, 1, 1};
+    void *bufs[TM_COUNT] = {gd.st[0], gd.st[1] ? gd.st[1] : gd.st[0], gd.k1, gd.k2};
+    for (int m = 0; m < TM_COUNT; ++m) {
+        if (((uintptr_t)bufs[m]) % 16) return false;
+        CUresult r = enc(&out[m], es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                         bufs[m], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return false;
+    }
+    return true;
 }
 
 size_t stage_smem_bytes(int prec, int order, int shape)

@@ -59,13 +59,27 @@ def kh(n: int, seed: int = 12345, noise: float = 1e-3, x0=0.0, y0=0.0, length=1.
     return np.stack([np.where(inside, 2.0, 1.0), np.where(inside, -0.5, 0.5), v, np.full((n, n), 2.5)])
 
 
-def riemann4(n: int, seed: int, x0=0.0, y0=0.0, length=1.0):
+def riemann4(n: int, seed: int, x0=0.0, y0=0.0, length=1.0, width: float = 2.0):
     """Four-quadrant Riemann problem; quadrant q = (x >= xm) + 2 (y >= ym)
-    takes draws 4q..4q+3 of stream `seed` for rho, u, v, p."""
+    takes draws 4q..4q+3 of stream `seed` for rho, u, v, p.  The interfaces
+    are tanh-smoothed over `width` cells (0 = sharp jumps), blending the four
+    quadrant states bilinearly."""
     X, Y = centers(n, x0, y0, length)
-    q = (X >= x0 + 0.5 * length).astype(np.uint64) + 2 * (Y >= y0 + 0.5 * length).astype(np.uint64)
-    d = [unit_draw(seed, 4 * q + m) for m in range(4)]
-    return np.stack([0.1 + 1.9 * d[0], -1 + 2 * d[1], -1 + 2 * d[2], 0.1 + 1.9 * d[3]])
+    h = length / n
+    xm, ym = x0 + 0.5 * length, y0 + 0.5 * length
+    if width > 0:
+        wx = 0.5 * (1 + np.tanh((X - xm) / (width * h)))
+        wy = 0.5 * (1 + np.tanh((Y - ym) / (width * h)))
+    else:
+        wx = (X >= xm).astype(float)
+        wy = (Y >= ym).astype(float)
+    wq = [(1 - wx) * (1 - wy), wx * (1 - wy), (1 - wx) * wy, wx * wy]
+    out = np.zeros((4, n, n))
+    lo_hi = [(0.1, 1.9), (-1.0, 2.0), (-1.0, 2.0), (0.1, 1.9)]
+    for q in range(4):
+        for m, (a, b) in enumerate(lo_hi):
+            out[m] += wq[q] * (a + b * unit_draw(seed, 4 * q + m))
+    return out
 
 
 def sod(n: int, length=1.0):
@@ -103,3 +117,21 @@ def rel_linf(a: np.ndarray, b: np.ndarray) -> float:
         s = np.max(np.abs(b[q]))
         out = max(out, float(np.max(np.abs(a[q] - b[q])) / (s if s > 0 else 1.0)))
     return out
+
+
+def smooth(n: int, seed: int, x0=0.0, y0=0.0, length=1.0):
+    """Smooth periodic random state (sums of a few Fourier modes): a
+    well-conditioned input for tolerance checks at any resolution."""
+    rng = np.random.default_rng(seed)
+    X, Y = centers(n, x0, y0, length)
+    kx = 2 * np.pi / length
+
+    def field(base, amp):
+        f = np.full((n, n), base)
+        for _ in range(3):
+            a, b = rng.integers(1, 4, 2)
+            ph = rng.uniform(0, 2 * np.pi)
+            f = f + amp * rng.uniform(0.3, 1.0) * np.sin(a * kx * (X - x0) + b * kx * (Y - y0) + ph)
+        return f
+
+    return np.stack([field(1.0, 0.2), field(0.0, 0.5), field(0.0, 0.5), field(1.0, 0.2)])

@@ -1,0 +1,172 @@
+"""The three forms beside the plain method, on the GPU through the C ABI:
+
+* precision: FP32 reconstruction/flux/divergence with a compensated hi/lo
+  FP32 conserved state, against the FP64 path (itself pinned to the oracle);
+* batching: many uneven grids in one persistent launch per stage -- each
+  instance's result equals the same grid advanced alone;
+* serving: a request stream through the continuous-batching loop -- every
+  request finishes, and its result is the one it gets alone.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import fvstuff_b200 as F
+from cases import kh, prim_to_cons, rel_linf, riemann4, smooth, vortex
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l1(a, b):
+    return float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
+
+
+def _run(prec, w, steps, **kw):
+    s = F.Solver(w.shape[-1], precision=prec, **kw)
+    s.set_state(w, interior=True)
+    s.step(steps)
+    st = s.sync()
+    assert st.status == 0 and st.steps == steps
+    return s, s.get_state(layout="cons", interior=True), st
+
+
+def test_f32c_vortex_against_f64():
+    """Moving isentropic vortex, periodic [-5,5]^2 at 128^2, 300 steps at CFL
+    0.5: density within 1e-6 relative L1 of the FP64 run."""
+    n, steps = 128, 300
+    w = vortex(n)
+    kw = dict(bc="periodic", x0=-5, y0=-5, length=10.0, cfl=0.5)
+    _, c64, s64 = _run("f64", w, steps, **kw)
+    _, c32, s32 = _run("f32c", w, steps, **kw)
+    e_rho = rel_l1(c32[0], c64[0])
+    e_inf = rel_linf(c32, c64)
+    print("f32c vs f64 vortex 128^2 x %d: rel L1(rho) %.3e, rel Linf(cons) %.3e, t %.9f / %.9f"
+          % (steps, e_rho, e_inf, s32.t, s64.t))
+    assert e_rho <= 1e-6
+    assert abs(s32.t - s64.t) <= 1e-6 * s64.t
+
+
+def test_f32c_kh_short_against_f64():
+    n, steps = 256, 100
+    w = kh(n)
+    _, c64, _ = _run("f64", w, steps, bc="periodic", cfl=0.5)
+    _, c32, _ = _run("f32c", w, steps, bc="periodic", cfl=0.5)
+    e = [rel_l1(c32[q], c64[q]) for q in range(4)]
+    print("f32c vs f64 KH 256^2 x %d: rel L1 rho %.2e rhou %.2e rhov %.2e E %.2e" % (steps, *e))
+    assert e[0] <= 1e-6
+
+
+def test_f32c_hilo_is_normalised_and_conservative():
+    n = 64
+    s = F.Solver(n, precision="f32c", bc="periodic")
+    s.set_state(smooth(n, seed=3), interior=True)
+    a = s.stats().sums
+    s.step(50)
+    b = s.stats().sums
+    hi, lo = s.get_state_hilo()
+    # |lo| <= ulp(hi)/2: the pair is a normalised double-float
+    assert np.all(np.abs(lo) <= np.spacing(np.abs(hi)) * 0.5 + 1e-45)
+    drift = [abs(b[q] - a[q]) / max(abs(a[q]), 1.0) for q in range(4)]
+    print("f32c conserved-sum drift after 50 steps:", drift)
+    assert max(drift) <= 1e-7
+
+
+def test_f32c_graph_and_direct_agree():
+    n = 48
+    w = riemann4(n, seed=2)
+    a = F.Solver(n, precision="f32c", bc="transmissive")
+    b = F.Solver(n, precision="f32c", bc="transmissive")
+    b.set_graph(False)
+    for s in (a, b):
+        s.set_state(w, interior=True)
+        s.step(9)   # odd: exercises the graph pair plus one direct step
+    assert np.array_equal(a.get_state(interior=True), b.get_state(interior=True))
+    a.advance(0.05)
+    b.advance(0.05)
+    assert np.array_equal(a.get_state(interior=True), b.get_state(interior=True))
+
+
+# --- batched form -------------------------------------------------------------
+
+def _desc(n, seed, t_end):
+    c = F.case_params("riemann4", 0.0, 0.0, 1.0, seed=seed)
+    return F.Batch.desc(n, c, t_end, bc="transmissive", cfl=0.5), c
+
+
+@pytest.mark.parametrize("prec", ["f32c", "f64"])
+def test_batch_instances_match_alone(prec):
+    sizes = [64, 96, 33, 128, 50, 160]
+    b = F.Batch(precision=prec)
+    ids, cases = [], []
+    for k, n in enumerate(sizes):
+        d, c = _desc(n, 100 + k, 0.05 + 0.01 * k)
+        ids.append(b.add(d))
+        cases.append((n, c, d.t_end))
+    done = set()
+    for _ in range(400):
+        b.run(8)
+        done.update(b.poll())
+        if len(done) == len(sizes):
+            break
+    assert done == set(ids)
+    for iid, (n, c, t_end) in zip(ids, cases):
+        st = b.stats(iid)
+        assert st.status == 0 and st.t == pytest.approx(t_end, rel=0, abs=1e-12)
+        got = b.get_state(iid, n)
+        s = F.Solver(n, precision=prec, bc="transmissive", cfl=0.5)
+        s.init_case(c)
+        s.advance(t_end)
+        alone = s.get_state(interior=True)
+        assert s.sync().steps == st.steps
+        assert np.array_equal(got, alone), (iid, n, np.max(np.abs(got - alone)))
+    for iid in ids:
+        b.remove(iid)
+    assert b.bytes_in_use() == 0
+
+
+def test_batch_join_midway_and_budget():
+    b = F.Batch(precision="f32c", hbm_budget=F.Batch(precision="f32c").instance_bytes(64) * 2)
+    d1, _ = _desc(64, 1, 0.04)
+    d2, c2 = _desc(64, 2, 0.03)
+    d3, _ = _desc(64, 3, 0.03)
+    i1 = b.add(d1)
+    b.run(3)
+    i2 = b.add(d2)  # joins while i1 is mid-run
+    with pytest.raises(F.FvbError) as e:
+        b.add(d3)
+    assert e.value.status == F._lib.ERR_NOMEM
+    done = set()
+    for _ in range(200):
+        b.run(4)
+        done.update(b.poll())
+        if done == {i1, i2}:
+            break
+    assert done == {i1, i2}
+    s = F.Solver(64, precision="f32c", bc="transmissive", cfl=0.5)
+    s.init_case(c2)
+    s.advance(0.03)
+    assert np.array_equal(b.get_state(i2, 64), s.get_state(interior=True))
+    b.remove(i1)
+    i3 = b.add(d3)  # fits once i1's memory is released
+    assert i3 >= 0
+
+
+# --- serving loop ---------------------------------------------------------------
+
+def test_serve_stream_matches_alone():
+    rng = np.random.default_rng(0)
+    reqs = []
+    t = 0.0
+    for k in range(12):
+        t += rng.exponential(1 / 200.0)
+        n = int(rng.choice([32, 48, 64, 80]))
+        d, _ = _desc(n, 500 + k, float(rng.uniform(0.02, 0.06)))
+        reqs.append((t, d))
+    res, wall = F.serve_run(reqs, precision="f32c", steps_per_round=4)
+    assert all(r["status"] == 0 and r["finished"] >= r["admitted"] >= 0 for r in res)
+    for (arr, d), r in zip(reqs, res):
+        assert r["admitted"] >= arr - 1e-3
+        assert abs(r["t"] - d.t_end) <= 1e-12
+    lat = sorted(r["finished"] - r["arrival"] for r in res)
+    print("serve: %d requests in %.3f s, p50 %.4f s p99 %.4f s" % (len(res), wall, lat[len(lat) // 2], lat[-1]))
