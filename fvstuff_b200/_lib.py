@@ -83,6 +83,8 @@ _SIG = {
     "fvb_apply_bc": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P]),
     "fvb_rk3_stage": (C.c_int, [C.c_int, _P, _P, _P, _P, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, _P]),
     "fvb_max": (C.c_int, [_P, C.c_size_t, _P, C.c_int, _P]),
+    "fvb_step_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                   C.c_int, C.c_double, C.c_double, _P, C.POINTER(Stats)]),
     "fvb_batch_create": (C.c_int, [C.POINTER(BatchConfig), C.POINTER(_P)]),
     "fvb_batch_destroy": (None, [_P]),
     "fvb_batch_instance_bytes": (C.c_size_t, [_P, C.c_int]),

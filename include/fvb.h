@@ -181,6 +181,21 @@ FVB_API fvb_status fvb_rk3_stage(int stage, void *Uo, const void *U0, const void
  *                                          replaces reduce_max/gpu_max, fv_up7_ducros_2d.cu:593-612 */
 FVB_API fvb_status fvb_max(const void *x, size_t n, void *out_dev, int dtype, void *stream);
 
+/* Up to nsteps SSP-RK3 steps (UP7 + Ducros, FP64) of a caller-held padded
+ * primitive state Qp (device, IDX_P layout, n <= 512, n + 8 <= np <= 520),
+ * starting at time t0 and stopping at t_stop, WITHOUT allocating device
+ * memory: for callers that cannot call cudaMalloc, e.g. an application whose
+ * device memory belongs to its own pool allocator or is fixed at start-up.
+ * The stage buffers and step control live in one fixed __device__ array of
+ * the library (about 17 MB, held on every GPU that loads libfvb.so), so
+ * calls that overlap on the GPU race with each other.  The ghost ring of Qp
+ * is refilled.  The first call on a device looks up the array's address;
+ * make that first call before any stream capture on that device.  When st
+ * is non-null the call waits for the stream and fills it.  No counterpart
+ * in the reference. */
+FVB_API fvb_status fvb_step_noalloc(double *Qp, int n, int np, double h, double cfl, double gamma, int bc_x,
+                                    int bc_y, int nsteps, double t0, double t_stop, void *stream, fvb_stats *st);
+
 /* ---- batched form: many uneven grids in one persistent launch per stage -- */
 
 typedef struct fvb_batch_config {
