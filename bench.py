@@ -47,6 +47,14 @@ def parse():
     p.add_argument("--no-forms", action="store_true", help="skip the extra FP32c measurement")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--mode", default="plain", choices=["plain", "batched", "serve", "large"],
+                   help="plain: the headline line; batched / serve / large: the other configurations")
+    p.add_argument("--instances", type=int, default=512, help="batched: number of grids")
+    p.add_argument("--plain-sample", type=int, default=32, help="batched: grids timed on the plain FP64 path")
+    p.add_argument("--requests", type=int, default=48, help="serve: requests in the stream")
+    p.add_argument("--rate", type=float, default=200.0, help="serve: mean arrivals per second")
+    p.add_argument("--max-n", type=int, default=2048, help="serve: largest grid side")
+    p.add_argument("--steps-per-round", type=int, default=16, help="serve: batch steps between admissions")
     return p.parse_args()
 
 
@@ -303,10 +311,194 @@ def run_gpu(args):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# the other configurations: batched (3), serving (4), large grid (5)
+# ---------------------------------------------------------------------------
+def riemann_instances(count, seed=2024):
+    """`count` four-quadrant Riemann problems, N uniform in {64, 96, ..., 512},
+    quadrant states from per-instance seeds, transmissive, t_end 0.25."""
+    import fvstuff_b200 as F
+    rng = np.random.default_rng(seed)
+    sizes = list(range(64, 513, 32))
+    out = []
+    for k in range(count):
+        n = int(rng.choice(sizes))
+        c = F.case_params("riemann4", 0.0, 0.0, 1.0, seed=int(rng.integers(1, 2 ** 62)))
+        out.append((n, c))
+    return out
+
+
+def advance_counted(s, t_end):
+    """fvb_advance; a grid that trips the blow-up / dt-underflow guard (as the
+    reference's own loop does, fv_up7_ducros_2d.cu:997-1007) stops there and
+    still counts the steps it made."""
+    import fvstuff_b200 as F
+    try:
+        s.advance(t_end)
+    except F.FvbError as e:
+        if e.status not in (F._lib.ERR_BLOWUP, F._lib.ERR_DT_UNDERFLOW):
+            raise
+    return s.sync()
+
+
+def run_plain_f64_alone(F, insts, t_end):
+    """The plain FP64 path, one grid at a time; returns (cell-stages, seconds,
+    grids stopped by the guard)."""
+    import torch
+    work, sec, bad = 0.0, 0.0, 0
+    for n, c in insts:
+        s = F.Solver(n, bc="transmissive", cfl=0.5, precision="f64")
+        s.init_case(c)
+        s.sync()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = advance_counted(s, t_end)
+        sec += time.perf_counter() - t0
+        work += 3.0 * n * n * st.steps
+        bad += st.status != 0
+        s.close()
+    return work, sec, bad
+
+
+def run_batched(args):
+    import torch
+
+    import fvstuff_b200 as F
+    count = args.instances
+    insts = riemann_instances(count)
+    t_end = 0.25
+    b = F.Batch(precision="f32c")
+    ids = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for n, c in insts:
+        ids[b.add(F.Batch.desc(n, c, t_end, bc="transmissive", cfl=0.5))] = n
+    done = set()
+    while len(done) < len(ids):
+        b.run(16)
+        done.update(b.poll())
+    sec = time.perf_counter() - t0
+    work, bad = 0.0, 0
+    for iid, n in ids.items():
+        st = b.stats(iid)
+        bad += st.status != 0
+        work += 3.0 * n * n * st.steps
+    b.close()
+    value = work / sec
+    # the plain FP64 form on the same grids one at a time: a seeded sample of
+    # them, the rate scaled to the sample's own work
+    sample = insts[:: max(1, count // args.plain_sample)]
+    pw, ps, pbad = run_plain_f64_alone(F, sample, t_end)
+    line = {"metric": METRIC, "value": value, "unit": "cell-stage updates/s", "n_gpus": 1, "steps": None,
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
+            "data": "synthetic", "mode": "batched",
+            "config": {"workload": "%d four-quadrant Riemann problems, N in {64..512} step 32, transmissive, "
+                                   "t=0.25, CFL 0.5, one persistent launch per RK stage (graph-replayed)" % count,
+                       "instances": count,
+                       "failed": bad, "failed_means": "stopped by the blow-up / dt-underflow guard of the "
+                                                     "reference scheme before t_end; their steps count"},
+            "seconds": sec, "cell_stages": work,
+            "plain_f64_one_at_a_time": {"value": pw / ps, "instances_sampled": len(sample), "seconds": ps,
+                                        "failed": pbad},
+            "batched_f32c_vs_plain_f64": value / (pw / ps)}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    import torch
+
+    import fvstuff_b200 as F
+    rng = np.random.default_rng(7)
+    reqs, t = [], 0.0
+    for k in range(args.requests):
+        t += rng.exponential(1.0 / args.rate)
+        n = int(round(math.exp(rng.uniform(math.log(128), math.log(args.max_n)))))
+        t_end = float(rng.uniform(0.1, 1.0))
+        if rng.random() < 0.5:
+            c = F.case_params("vortex", -5.0, -5.0, 10.0)
+            d = F.Batch.desc(n, c, t_end, bc="periodic", x0=-5.0, y0=-5.0, length=10.0, cfl=0.5)
+        else:
+            c = F.case_params("riemann4", 0.0, 0.0, 1.0, seed=int(rng.integers(1, 2 ** 62)))
+            d = F.Batch.desc(n, c, t_end, bc="transmissive", cfl=0.5)
+        reqs.append((t, d))
+    torch.cuda.synchronize()
+    res, wall = F.serve_run(reqs, precision="f32c", hbm_budget=150 << 30, steps_per_round=args.steps_per_round)
+    lat = sorted(r["finished"] - r["arrival"] for r in res)
+    work = sum(3.0 * d.n * d.n * r["steps"] for (_, d), r in zip(reqs, res))
+    # the same requests one at a time on the plain FP64 path, back to back
+    t0 = time.perf_counter()
+    seq_lat, clock = [], 0.0
+    for (arr, d), r in zip(reqs, res):
+        s = F.Solver(d.n, bc={0: "reflect", 1: "periodic", 2: "transmissive"}[d.bc_x], x0=d.x0, y0=d.y0,
+                     length=d.length, cfl=d.cfl, precision="f64")
+        s.init_case(d.ic)
+        a = time.perf_counter()
+        advance_counted(s, d.t_end)
+        clock = max(clock, arr) + (time.perf_counter() - a)
+        seq_lat.append(clock - arr)
+        s.close()
+    seq_wall = time.perf_counter() - t0
+    seq_lat.sort()
+    pct = lambda v, q: v[min(len(v) - 1, int(q * len(v)))]
+    line = {"metric": METRIC, "value": work / wall, "unit": "cell-stage updates/s", "n_gpus": 1,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32c", "data": "synthetic",
+            "mode": "serve",
+            "config": {"workload": "Poisson stream, %d requests at %.0f/s, vortex or seeded Riemann, N log-uniform "
+                                   "in [128, %d], t_end U[0.1, 1], 150 GB HBM budget" % (args.requests, args.rate,
+                                                                                        args.max_n)},
+            "p50_s": pct(lat, 0.5), "p99_s": pct(lat, 0.99), "wall_s": wall,
+            "failed": sum(r["status"] != 0 for r in res),
+            "sequential_plain_f64": {"value": work / seq_wall, "p50_s": pct(seq_lat, 0.5),
+                                     "p99_s": pct(seq_lat, 0.99), "wall_s": seq_wall}}
+    print(json.dumps(line), flush=True)
+
+
+def run_large(args):
+    import torch
+
+    import fvstuff_b200 as F
+    n, K = args.n, args.steps
+    out = {}
+    for prec in ("f32c", "f64"):
+        stream = torch.cuda.Stream()
+        s = F.Solver(n, bc="periodic", cfl=0.5, precision=prec, stream=stream.cuda_stream)
+        s.init_case("kh")
+        a = s.stats().sums
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clk:
+            e0.record(stream)
+            s.step(K)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = s.stats()
+        drift = [(st.sums[q] - a[q]) / abs(a[q]) for q in (0, 3)]
+        hbm, _ = peaks()
+        gbs = BYTES_PER_CELL_STAGE[prec] * n * n * 3 * K / (ms / 1e3) / 1e9
+        out[prec] = {"value": 3.0 * n * n * K / (ms / 1e3), "ms_per_step": ms / K, "t": st.t, "steps": st.steps,
+                     "status": st.status, "mass_drift": drift[0], "energy_drift": drift[1],
+                     "achieved_gbs": gbs, "roofline_frac": gbs / hbm, "clocks": clk.summary()}
+        s.close()
+    line = {"metric": METRIC, "value": out["f32c"]["value"], "unit": "cell-stage updates/s", "n_gpus": 1,
+            "steps": K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
+            "data": "synthetic", "mode": "large",
+            "config": {"workload": "kelvin-helmholtz %dx%d periodic, %d SSP-RK3 steps at CFL 0.5" % (n, n, K)},
+            "forms": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.mode == "batched":
+        run_batched(args)
+    elif args.mode == "serve":
+        run_serve(args)
+    elif args.mode == "large":
+        run_large(args)
     else:
         run_gpu(args)
 

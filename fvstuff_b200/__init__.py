@@ -192,6 +192,13 @@ class Solver:
         check(lib().fvb_stats_sums(self._h, C.byref(s)), "fvb_stats_sums")
         return Stats.from_c(s)
 
+    def save(self, path) -> None:
+        """Exact checkpoint (state, time, steps, next-dt wave speed)."""
+        check(lib().fvb_save(self._h, str(path).encode()), "fvb_save")
+
+    def load(self, path) -> None:
+        check(lib().fvb_load(self._h, str(path).encode()), "fvb_load")
+
     def set_graph(self, enable: bool) -> None:
         check(lib().fvb_set_graph(self._h, int(bool(enable))), "fvb_set_graph")
 

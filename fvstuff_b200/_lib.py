@@ -8,7 +8,10 @@ from __future__ import annotations
 import ctypes as C
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "libfvb.so"
+import os
+
+# the in-tree build; FVB_LIBRARY may name another build of the same sources
+LIB_PATH = Path(os.environ.get("FVB_LIBRARY", Path(__file__).resolve().parent / "libfvb.so"))
 
 # enums (include/fvb.h)
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_BLOWUP, ERR_DT_UNDERFLOW, ERR_NOT_FOUND, ERR_TIMEOUT = range(8)
@@ -74,6 +77,8 @@ _SIG = {
     "fvb_set_state": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int]),
     "fvb_get_state": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int]),
     "fvb_get_state_hilo": (C.c_int, [_P, _P, _P]),
+    "fvb_save": (C.c_int, [_P, C.c_char_p]),
+    "fvb_load": (C.c_int, [_P, C.c_char_p]),
     "fvb_step": (C.c_int, [_P, C.c_int, C.c_double]),
     "fvb_advance": (C.c_int, [_P, C.c_double, C.c_int64, C.c_int]),
     "fvb_sync": (C.c_int, [_P, C.POINTER(Stats)]),

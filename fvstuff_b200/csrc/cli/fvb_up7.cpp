@@ -1,0 +1,225 @@
+// fvb_up7 -- command-line drop-in for fvStuff's fv_up7 (fv_up7_ducros_2d.cu
+// main, :886-1067) on libfvb.
+//
+//   fvb_up7 [N] [--cfl C] [--t-end T] [--case sod|vortex|kh|riemann4]
+//           [--gamma G] [--bc reflect|periodic|transmissive] [--order 3|5|7]
+//           [--precision f64|f32|f32c] [--frames F] [--prefix P] [--seed S]
+//           [--bin] [--no-ppm] [--save FILE] [--resume FILE]
+//
+// Defaults are the reference's: N = 400, CFL 0.40, t_end 1, circular Sod
+// with reflecting walls on [0,1]^2, UP7 (FP64 arithmetic here), 10 frames
+// written as <prefix>_%04d.ppm (2N x 2N composite: density, vorticity,
+// Ducros sensor, |v|), frame 99 on blow-up.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fvb.h"
+#include "fvb_io.h"
+
+namespace {
+
+struct Args {
+    int n = 400, order = 7, frames = 10, precision = FVB_PREC_F64, bc = -1, kase = FVB_CASE_SOD;
+    double cfl = 0.40, t_end = 1.0, gamma = 1.4;
+    long long seed = -1;
+    std::string prefix = "sod", save, resume;
+    bool bin = false, ppm = true;
+};
+
+int parse_enum(const char *v, const char *const *names, int count, const char *what)
+{
+    for (int k = 0; k < count; ++k)
+        if (!std::strcmp(v, names[k])) return k;
+    std::fprintf(stderr, "unknown %s '%s'\n", what, v);
+    std::exit(2);
+}
+
+Args parse(int argc, char **argv)
+{
+    static const char *cases[] = {"sod", "vortex", "kh", "riemann4"};
+    static const char *bcs[] = {"reflect", "periodic", "transmissive"};
+    static const char *precs[] = {"f64", "f32", "f32c"};
+    Args a;
+    for (int k = 1; k < argc; ++k) {
+        std::string s = argv[k];
+        auto val = [&]() -> const char * {
+            if (k + 1 >= argc) { std::fprintf(stderr, "%s needs a value\n", s.c_str()); std::exit(2); }
+            return argv[++k];
+        };
+        if (s == "--cfl") a.cfl = std::atof(val());
+        else if (s == "--t-end") a.t_end = std::atof(val());
+        else if (s == "--case") a.kase = parse_enum(val(), cases, 4, "case");
+        else if (s == "--gamma") a.gamma = std::atof(val());
+        else if (s == "--bc") a.bc = parse_enum(val(), bcs, 3, "boundary condition");
+        else if (s == "--order") a.order = std::atoi(val());
+        else if (s == "--precision") a.precision = parse_enum(val(), precs, 3, "precision");
+        else if (s == "--frames") a.frames = std::atoi(val());
+        else if (s == "--prefix") a.prefix = val();
+        else if (s == "--seed") a.seed = std::atoll(val());
+        else if (s == "--bin") a.bin = true;
+        else if (s == "--no-ppm") a.ppm = false;
+        else if (s == "--save") a.save = val();
+        else if (s == "--resume") a.resume = val();
+        else if (s[0] != '-') a.n = std::atoi(s.c_str());
+        else { std::fprintf(stderr, "unknown option %s\n", s.c_str()); std::exit(2); }
+    }
+    if (a.bc < 0) a.bc = (a.kase == FVB_CASE_SOD) ? FVB_BC_REFLECT : (a.kase == FVB_CASE_RIEMANN4 ? FVB_BC_TRANSMISSIVE : FVB_BC_PERIODIC);
+    return a;
+}
+
+struct Frames {
+    int N, g, Np;
+    double h;
+    float rho_lo, rho_hi;
+    std::vector<float> Q, rho, p, sd, vort, vmag;
+    explicit Frames(int n, int gg, double hh) : N(n), g(gg), Np(n + 2 * gg), h(hh)
+    {
+        Q.resize((size_t)4 * Np * Np);
+        for (auto *v : {&rho, &p, &sd, &vort, &vmag}) v->resize((size_t)N * N);
+    }
+    float at(int q, int jp, int ip) const { return Q[(size_t)q * Np * Np + (size_t)jp * Np + ip]; }
+    // Ducros cell sensor (max of its 4 faces), 6th-order vorticity and |v|
+    //                                   fv_up7_ducros_2d.cu:511-526, :800-829
+    void derive()
+    {
+        auto ducros = [](float pa, float pb) {
+            float dp = pb - pa, ps = pb + pa;
+            return dp * dp / (dp * dp + 0.1f * ps * ps);
+        };
+        static const float coeff[6] = {-1.f, 9.f, -45.f, 45.f, -9.f, 1.f};
+        static const int off[6] = {-3, -2, -1, 1, 2, 3};
+        for (int j = 0; j < N; ++j)
+            for (int i = 0; i < N; ++i) {
+                const int jp = j + g, ip = i + g;
+                const size_t k = (size_t)j * N + i;
+                rho[k] = at(0, jp, ip);
+                p[k] = at(3, jp, ip);
+                sd[k] = std::fmax(std::fmax(ducros(at(3, jp, ip), at(3, jp, ip + 1)), ducros(at(3, jp, ip - 1), at(3, jp, ip))),
+                                  std::fmax(ducros(at(3, jp, ip), at(3, jp + 1, ip)), ducros(at(3, jp - 1, ip), at(3, jp, ip))));
+                float dvdx = 0.f, dudy = 0.f;
+                for (int d = 0; d < 6; ++d) {
+                    if (g >= 3) {
+                        dvdx += coeff[d] * at(2, jp, ip + off[d]);
+                        dudy += coeff[d] * at(1, jp + off[d], ip);
+                    }
+                }
+                vort[k] = (dvdx - dudy) / (60.0f * (float)h);
+                const float u = at(1, jp, ip), v = at(2, jp, ip);
+                vmag[k] = std::sqrt(u * u + v * v);
+            }
+    }
+};
+
+bool write_frame(fvb_solver *s, Frames &F, const Args &a, int idx)
+{
+    if (fvb_get_state(s, F.Q.data(), FVB_LAYOUT_PRIM, FVB_F32, FVB_HOST, 0)) {
+        std::fprintf(stderr, "state read failed: %s\n", fvb_last_error());
+        return false;
+    }
+    F.derive();
+    char fn[512];
+    if (a.ppm) {
+        float wmax = 1e-10f, vmax = 1e-10f;
+        for (size_t k = 0; k < F.vort.size(); ++k) {
+            wmax = std::max(wmax, std::fabs(F.vort[k]));
+            vmax = std::max(vmax, F.vmag[k]);
+        }
+        std::snprintf(fn, sizeof fn, "%s_%04d.ppm", a.prefix.c_str(), idx);
+        fvbio::write_ppm_2x2(fn, {F.rho.data(), F.rho_lo, F.rho_hi, fvbio::PLASMA}, {F.vort.data(), -wmax, wmax, fvbio::BWR},
+                             {F.sd.data(), 0.f, 1.f, fvbio::HOT}, {F.vmag.data(), 0.f, vmax, fvbio::VIRIDIS}, F.N);
+    }
+    if (a.bin) {
+        std::snprintf(fn, sizeof fn, "%s_%04d.bin", a.prefix.c_str(), idx);
+        fvbio::write_bin(fn, F.rho.data(), F.p.data(), F.N);
+    }
+    return true;
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    Args a = parse(argc, argv);
+    fvb_config cfg;
+    fvb_config_default(&cfg, a.n);
+    cfg.order = a.order;
+    cfg.precision = a.precision;
+    cfg.bc_x = cfg.bc_y = a.bc;
+    cfg.cfl = a.cfl;
+    cfg.gamma = a.gamma;
+    if (a.kase == FVB_CASE_VORTEX) { cfg.x0 = cfg.y0 = -5.0; cfg.length = 10.0; }
+    fvb_solver *s = nullptr;
+    if (fvb_create(&cfg, &s)) { std::fprintf(stderr, "fvb_create: %s\n", fvb_last_error()); return 1; }
+    const int g = fvb_ghost_width(s);
+    const double h = cfg.length / a.n;
+    static const char *names[] = {"Circular Sod", "Isentropic vortex", "Kelvin-Helmholtz", "Four-quadrant Riemann"};
+    std::printf("========================================================\n");
+    std::printf("  Device  : %s\n", fvb_version());
+    std::printf("  UP%d+HLLC+Ducros FV 2D  --  %s\n", a.order, names[a.kase]);
+    std::printf("  n=%dx%d  Np=%d  h=%.5f  CFL=%.2f  order=%d\n", a.n, a.n, a.n + 2 * g, h, a.cfl, a.order);
+    std::printf("========================================================\n");
+
+    fvb_case c;
+    fvb_case_default(&c, a.kase, cfg.x0, cfg.y0, cfg.length);
+    if (a.seed >= 0) c.seed = (uint64_t)a.seed;
+    if (fvb_init_case(s, &c)) { std::fprintf(stderr, "init: %s\n", fvb_last_error()); return 1; }
+    Frames F(a.n, g, h);
+    // density colour scale fixed to the initial extremes for the whole run
+    // (the reference fixes 0.125 .. 10.1 for its Sod case, :932)
+    if (a.kase == FVB_CASE_SOD) { F.rho_lo = 0.125f; F.rho_hi = 10.1f; }
+    else {
+        fvb_get_state(s, F.Q.data(), FVB_LAYOUT_PRIM, FVB_F32, FVB_HOST, 0);
+        F.derive();
+        auto mm = std::minmax_element(F.rho.begin(), F.rho.end());
+        F.rho_lo = *mm.first; F.rho_hi = *mm.second;
+    }
+    if (!a.resume.empty()) {
+        if (fvb_load(s, a.resume.c_str())) { std::fprintf(stderr, "resume: %s\n", fvb_last_error()); return 1; }
+    }
+    fvb_stats st;
+    fvb_sync(s, &st);
+    int frame = 1;
+    if (a.resume.empty() || st.t == 0.0) write_frame(s, F, a, 0);
+    else while (frame <= a.frames && st.t >= frame * a.t_end / a.frames - 1e-12) ++frame;
+    double t_next = frame * a.t_end / a.frames;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto elapsed = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    long long last_print = st.steps;
+    while (st.t < a.t_end) {
+        const double target = std::min(t_next, a.t_end);
+        // at most 50 steps per call so progress prints like the reference's
+        int chunk = (int)(50 - (st.steps % 50));
+        if (fvb_step(s, chunk, target) || fvb_sync(s, &st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }
+        if (st.status) {
+            std::fprintf(stderr, "  %s at step %lld t=%.6f lam_max=%.3e -- writing blow-up frame\n",
+                         st.status == FVB_ERR_BLOWUP ? "NaN/Inf lam_max" : "dt underflow", (long long)st.steps, st.t,
+                         st.lam_max);
+            write_frame(s, F, a, 99);
+            break;
+        }
+        if (st.t >= t_next - 1e-12 && frame <= a.frames) {
+            std::printf("  frame %2d/%d  step %5lld  t=%.5f  elapsed=%.1fs\n", frame, a.frames, (long long)st.steps,
+                        st.t, elapsed());
+            std::fflush(stdout);
+            write_frame(s, F, a, frame);
+            ++frame;
+            t_next = frame * a.t_end / a.frames;
+        } else if (st.steps / 50 != last_print / 50) {
+            const double el = elapsed();
+            std::printf("  step %5lld  t=%.5f  dt=%.3e  elapsed=%.1fs  ETA=%.0fs\n", (long long)st.steps, st.t, st.dt,
+                        el, st.t > 0 ? (a.t_end - st.t) / st.t * el : 0.0);
+            std::fflush(stdout);
+        }
+        last_print = st.steps;
+    }
+    std::printf("  Done: %lld steps,  t=%.6f,  wall=%.2fs\n", (long long)st.steps, st.t, elapsed());
+    if (a.ppm) std::printf("  Frames written: %s_0000.ppm .. %s_%04d.ppm  (2x2 composite)\n", a.prefix.c_str(), a.prefix.c_str(), a.frames);
+    if (!a.save.empty() && fvb_save(s, a.save.c_str())) std::fprintf(stderr, "save: %s\n", fvb_last_error());
+    fvb_destroy(s);
+    return 0;
+}

@@ -142,6 +142,7 @@ struct fvb_solver {
     bool use_graph = false;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int graph_steps = 1;
+    bool keep = false;  // KEEP flux family: conserved FP64 state, g = 2
 };
 
 static fvb_status ensure_staging(fvb_solver *s)
@@ -169,6 +170,13 @@ static StageArgs stage_args(const fvb_solver *s, int stage, int parity)
 static cudaError_t enqueue_steps_direct(fvb_solver *s, int nsteps)
 {
     for (int k = 0; k < nsteps; ++k) {
+        if (s->keep) {
+            for (int stage = 1; stage <= 3; ++stage) {
+                cudaError_t e = keep_launch_stage(s->gd, stage, s->tiles, s->stream);
+                if (e != cudaSuccess) return e;
+            }
+            continue;
+        }
         for (int stage = 1; stage <= 3; ++stage) {
             StageArgs a = stage_args(s, stage, s->parity);
             cudaError_t e = launch_stage(s->prec, s->order, s->shape, a, s->ctas, s->stream);
@@ -223,6 +231,12 @@ static fvb_status refresh_after_state(fvb_solver *s, int buf_parity)
 {
     cudaError_t e;
     BufView v = view_of(s->gd);
+    if (s->keep) {
+        e = bc_fill<double>((double *)s->gd.st[0], v, s->gd.bcx, s->gd.bcy, s->stream);
+        if (e == cudaSuccess) e = keep_lam_into(s->gd, s->stream);
+        if (e == cudaSuccess) e = ctrl_set(s->ctrl, 0.0, 1, 0.0, s->cfg.cfl, s->cfg.length / s->n, s->stream);
+        return e == cudaSuccess ? FVB_OK : cuda_fail(e, "state refresh");
+    }
     if (s->internal == INT_PRIM64) e = bc_fill<double>((double *)s->gd.st[0], v, s->gd.bcx, s->gd.bcy, s->stream);
     else if (s->internal == INT_PRIM32) e = bc_fill<float>((float *)s->gd.st[0], v, s->gd.bcx, s->gd.bcy, s->stream);
     else {
@@ -271,14 +285,16 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
 {
     if (!cfg || !out) return fail(FVB_ERR_INVALID, "null argument");
     *out = nullptr;
-    if (cfg->flux == FVB_FLUX_KEEP) return keep_create(cfg, out);
-    if (cfg->flux != FVB_FLUX_UP_DUCROS) return fail(FVB_ERR_INVALID, "unknown flux %d", cfg->flux);
+    const bool keep = cfg->flux == FVB_FLUX_KEEP;
+    if (cfg->flux != FVB_FLUX_UP_DUCROS && !keep) return fail(FVB_ERR_INVALID, "unknown flux %d", cfg->flux);
     if (cfg->precision < 0 || cfg->precision > 2) return fail(FVB_ERR_INVALID, "unknown precision %d", cfg->precision);
-    if (!(cfg->order == 3 || cfg->order == 5 || cfg->order == 7))
+    if (keep && cfg->precision != FVB_PREC_F64)
+        return fail(FVB_ERR_INVALID, "the KEEP flux family runs in FP64 (as keep_fv_euler_2d.cu)");
+    if (!keep && !(cfg->order == 3 || cfg->order == 5 || cfg->order == 7))
         return fail(FVB_ERR_INVALID, "order must be 3, 5 or 7 (got %d)", cfg->order);
-    if (cfg->precision != FVB_PREC_F64 && cfg->order != 7)
+    if (!keep && cfg->precision != FVB_PREC_F64 && cfg->order != 7)
         return fail(FVB_ERR_INVALID, "orders 3 and 5 are built for FP64 only");
-    const int g = (cfg->order + 1) / 2;
+    const int g = keep ? 2 : (cfg->order + 1) / 2;
     if (cfg->n < g || cfg->n > 65536) return fail(FVB_ERR_INVALID, "n = %d out of range [%d, 65536]", cfg->n, g);
     for (int b : {cfg->bc_x, cfg->bc_y})
         if (b < 0 || b > 2) return fail(FVB_ERR_INVALID, "unknown boundary condition %d", b);
@@ -295,7 +311,8 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     s->order = cfg->order;
     s->g = g;
     s->n = cfg->n;
-    s->internal = prec_internal(s->prec);
+    s->keep = keep;
+    s->internal = keep ? INT_CONS64 : prec_internal(s->prec);
     s->G = make_geometry(cfg->n, g, s->prec);
     if (cfg->stream) s->stream = (cudaStream_t)cfg->stream;
     else {
@@ -325,6 +342,16 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     e = cudaMallocHost(&s->ctrl_host, sizeof(Ctrl));
     if (e != cudaSuccess) { fvb_destroy(s); return cuda_fail(e, "cudaMallocHost"); }
 
+    if (keep) {
+        // KEEP: plain loads into its own tile kernel, no graph variants
+        keep_tiles(s->n, s->gd.tiles_x, s->tiles);
+        s->graph_steps = 1;
+        s->use_graph = cfg->n <= 512;
+        e = ctrl_set(s->ctrl, 0.0, 1, 0.0, cfg->cfl, s->gd.h, s->stream);
+        if (e != cudaSuccess) { fvb_destroy(s); return cuda_fail(e, "step control"); }
+        *out = s;
+        return FVB_OK;
+    }
     s->shape = cfg->tile >= 0 ? cfg->tile : autotune_shape(s->prec, s->order, cfg->n);
     tile_dims(s->shape, s->n, s->gd.tiles_x, s->tiles);
     {
@@ -358,7 +385,6 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
 void fvb_destroy(fvb_solver *s)
 {
     if (!s) return;
-    if (s->cfg.flux == FVB_FLUX_KEEP) { keep_destroy(s); return; }
     if (s->stream) cudaStreamSynchronize(s->stream);
     drop_graphs(s);
     if (s->block) cudaFree(s->block);
@@ -375,7 +401,6 @@ int fvb_ghost_width(const fvb_solver *s) { return s ? s->g : 0; }
 fvb_status fvb_init_case(fvb_solver *s, const fvb_case *c)
 {
     if (!s || !c) return fail(FVB_ERR_INVALID, "null argument");
-    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_init_case(s, c);
     fvb_status st = ensure_staging(s);
     if (st) return st;
     cudaError_t e = init_case_prim64((double *)s->staging, s->n, s->cfg.x0, s->cfg.y0, s->gd.h, s->cfg.gamma, *c,
@@ -392,7 +417,6 @@ fvb_status fvb_init_case(fvb_solver *s, const fvb_case *c)
 fvb_status fvb_set_state(fvb_solver *s, const void *src, int layout, int dtype, int where, int interior_only)
 {
     if (!s || !src) return fail(FVB_ERR_INVALID, "null argument");
-    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_set_state(s, src, layout, dtype, where, interior_only);
     if ((layout != 0 && layout != 1) || (dtype != 0 && dtype != 1) || (where != 0 && where != 1))
         return fail(FVB_ERR_INVALID, "bad layout/dtype/where");
     ExtView ev{interior_only ? 1 : 0, s->g, s->G.np, layout, dtype};
@@ -422,7 +446,6 @@ fvb_status fvb_set_state(fvb_solver *s, const void *src, int layout, int dtype, 
 fvb_status fvb_get_state(fvb_solver *s, void *dst, int layout, int dtype, int where, int interior_only)
 {
     if (!s || !dst) return fail(FVB_ERR_INVALID, "null argument");
-    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_get_state(s, dst, layout, dtype, where, interior_only);
     if ((layout != 0 && layout != 1) || (dtype != 0 && dtype != 1) || (where != 0 && where != 1))
         return fail(FVB_ERR_INVALID, "bad layout/dtype/where");
     ExtView ev{interior_only ? 1 : 0, s->g, s->G.np, layout, dtype};
@@ -447,6 +470,85 @@ fvb_status fvb_get_state(fvb_solver *s, void *dst, int layout, int dtype, int wh
     return FVB_OK;
 }
 
+// checkpoint file: a fixed header, then the current state buffer(s) as
+// stored on the device (pitched padded planes), so a load is exact
+struct CkptHeader {
+    char magic[8];  // "FVBCKPT1"
+    int n, g, order, flux, precision, internal;
+    long long plane;
+    int pitch, xoff;
+    double t;
+    long long steps;
+    unsigned long long lam_bits;
+    int nbufs, pad;
+};
+
+fvb_status fvb_save(fvb_solver *s, const char *path)
+{
+    if (!s || !path) return fail(FVB_ERR_INVALID, "null argument");
+    fvb_stats st;
+    fvb_status r = fvb_sync(s, &st);
+    if (r) return r;
+    CkptHeader h{};
+    std::memcpy(h.magic, "FVBCKPT1", 8);
+    h.n = s->n; h.g = s->g; h.order = s->order; h.flux = s->cfg.flux; h.precision = s->prec;
+    h.internal = s->internal; h.plane = s->G.plane; h.pitch = s->G.pitch; h.xoff = s->G.xoff;
+    h.t = s->ctrl_host->t; h.steps = s->ctrl_host->step; h.lam_bits = s->ctrl_host->lam_acc;
+    h.nbufs = s->internal == INT_CONS_HILO ? 2 : 1;
+    const size_t bytes = (size_t)4 * s->G.plane * s->G.elem;
+    std::vector<char> buf(bytes);
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(FVB_ERR_INVALID, "cannot open %s for writing", path);
+    bool ok = std::fwrite(&h, sizeof h, 1, f) == 1;
+    void *src[2] = {s->gd.st[s->internal == INT_CONS_HILO ? s->parity : 0], s->gd.lo[s->parity]};
+    for (int b = 0; ok && b < h.nbufs; ++b) {
+        cudaError_t e = cudaMemcpy(buf.data(), src[b], bytes, cudaMemcpyDeviceToHost);
+        ok = e == cudaSuccess && std::fwrite(buf.data(), 1, bytes, f) == bytes;
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? FVB_OK : fail(FVB_ERR_INVALID, "writing %s failed", path);
+}
+
+fvb_status fvb_load(fvb_solver *s, const char *path)
+{
+    if (!s || !path) return fail(FVB_ERR_INVALID, "null argument");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(FVB_ERR_INVALID, "cannot open %s", path);
+    CkptHeader h{};
+    if (std::fread(&h, sizeof h, 1, f) != 1 || std::memcmp(h.magic, "FVBCKPT1", 8) != 0) {
+        std::fclose(f);
+        return fail(FVB_ERR_INVALID, "%s is not an fvb checkpoint", path);
+    }
+    if (h.n != s->n || h.g != s->g || h.order != s->order || h.flux != s->cfg.flux || h.precision != s->prec ||
+        h.internal != s->internal || h.plane != s->G.plane || h.pitch != s->G.pitch) {
+        std::fclose(f);
+        return fail(FVB_ERR_INVALID, "checkpoint %s was written by a solver of another configuration", path);
+    }
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) { std::fclose(f); return cuda_fail(e, "sync"); }
+    const size_t bytes = (size_t)4 * s->G.plane * s->G.elem;
+    std::vector<char> buf(bytes);
+    void *dst[2] = {s->gd.st[s->internal == INT_CONS_HILO ? s->parity : 0], s->gd.lo[s->parity]};
+    for (int b = 0; b < h.nbufs; ++b) {
+        if (std::fread(buf.data(), 1, bytes, f) != bytes) { std::fclose(f); return fail(FVB_ERR_INVALID, "%s is truncated", path); }
+        e = cudaMemcpy(dst[b], buf.data(), bytes, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { std::fclose(f); return cuda_fail(e, "restore"); }
+    }
+    std::fclose(f);
+    // the step control as it was: time, steps, and the wave-speed max
+    e = ctrl_set(s->ctrl, 0.0, 1, h.t, s->cfg.cfl, s->gd.h, s->stream);
+    Ctrl c{};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->ctrl_host, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "restore step control");
+    c = *s->ctrl_host;
+    c.step = h.steps;
+    c.lam_acc = h.lam_bits;
+    c.t = h.t;
+    e = cudaMemcpy(s->ctrl, &c, sizeof c, cudaMemcpyHostToDevice);
+    return e == cudaSuccess ? FVB_OK : cuda_fail(e, "restore step control");
+}
+
 fvb_status fvb_get_state_hilo(fvb_solver *s, float *hi, float *lo)
 {
     if (!s || !hi || !lo) return fail(FVB_ERR_INVALID, "null argument");
@@ -469,7 +571,6 @@ fvb_status fvb_get_state_hilo(fvb_solver *s, float *hi, float *lo)
 fvb_status fvb_step(fvb_solver *s, int nsteps, double t_stop)
 {
     if (!s || nsteps < 0) return fail(FVB_ERR_INVALID, "bad argument");
-    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_step(s, nsteps, t_stop);
     cudaError_t e = ctrl_set(s->ctrl, t_stop, 0, 0, 0, 0, s->stream);
     if (e == cudaSuccess) e = enqueue_steps(s, nsteps);
     if (e != cudaSuccess) return cuda_fail(e, "step launch");
@@ -479,7 +580,6 @@ fvb_status fvb_step(fvb_solver *s, int nsteps, double t_stop)
 fvb_status fvb_sync(fvb_solver *s, fvb_stats *st)
 {
     if (!s) return fail(FVB_ERR_INVALID, "null solver");
-    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_sync(s, st);
     cudaError_t e = cudaMemcpyAsync(s->ctrl_host, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) return cuda_fail(e, "sync");
@@ -525,7 +625,6 @@ fvb_status fvb_advance(fvb_solver *s, double t_stop, int64_t max_steps, int chun
 fvb_status fvb_stats_sums(fvb_solver *s, fvb_stats *st)
 {
     if (!s || !st) return fail(FVB_ERR_INVALID, "null argument");
-    if (s->cfg.flux == FVB_FLUX_KEEP) return keep_stats_sums(s, st);
     if (!s->sums_dev) {
         s->sums_blocks = 592;
         cudaError_t e = cudaMalloc(&s->sums_dev, sizeof(double) * 5 * s->sums_blocks);
@@ -553,7 +652,6 @@ fvb_status fvb_stats_sums(fvb_solver *s, fvb_stats *st)
 fvb_status fvb_set_graph(fvb_solver *s, int enable)
 {
     if (!s) return fail(FVB_ERR_INVALID, "null solver");
-    if (s->cfg.flux == FVB_FLUX_KEEP) return FVB_OK;
     cudaError_t e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) return cuda_fail(e, "sync");
     s->use_graph = enable != 0;

@@ -233,7 +233,12 @@ __global__ void import_kernel(const void *src, ExtView e, void *dst, void *dst_l
         for (int q = 0; q < 4; ++q)
             x[q] = e.dtype == FVB_F64 ? ld64<double>(src, es + q * eplane) : ld64<float>(src, es + q * eplane);
         long long d = (long long)(j + v.g) * v.pitch + (i + v.g) + v.xoff;
-        if (internal == INT_CONS_HILO) {
+        if (internal == INT_CONS64) {
+            double c[4];
+            if (e.layout == FVB_LAYOUT_PRIM) prim_to_cons64(x, c, gam);
+            else for (int q = 0; q < 4; ++q) c[q] = x[q];
+            for (int q = 0; q < 4; ++q) ((double *)dst)[d + q * v.plane] = c[q];
+        } else if (internal == INT_CONS_HILO) {
             double c[4];
             if (e.layout == FVB_LAYOUT_PRIM) prim_to_cons64(x, c, gam);
             else for (int q = 0; q < 4; ++q) c[q] = x[q];
@@ -271,9 +276,11 @@ __global__ void export_kernel(const void *src, const void *src_lo, BufView v, in
         const int jp = jj + off, ip = ii + off;
         long long s = (long long)jp * v.pitch + ip + v.xoff;
         double x[4];
-        if (internal == INT_CONS_HILO) {
+        if (internal == INT_CONS_HILO || internal == INT_CONS64) {
             for (int q = 0; q < 4; ++q)
-                x[q] = (double)((const float *)src)[s + q * v.plane] + (double)((const float *)src_lo)[s + q * v.plane];
+                x[q] = internal == INT_CONS64 ? ((const double *)src)[s + q * v.plane]
+                                              : (double)((const float *)src)[s + q * v.plane] +
+                                                    (double)((const float *)src_lo)[s + q * v.plane];
             if (e.layout == FVB_LAYOUT_PRIM) { double w[4]; cons_to_prim64(x, w, gam); for (int q = 0; q < 4; ++q) x[q] = w[q]; }
         } else {
             for (int q = 0; q < 4; ++q)
@@ -379,7 +386,9 @@ __global__ void sums_kernel(const void *st, const void *lo, BufView v, int inter
         const int j = (int)(k / n), i = (int)(k % n);
         long long s = (long long)(j + v.g) * v.pitch + (i + v.g) + v.xoff;
         double c[4];
-        if (internal == INT_CONS_HILO) {
+        if (internal == INT_CONS64) {
+            for (int q = 0; q < 4; ++q) c[q] = ((const double *)st)[s + q * v.plane];
+        } else if (internal == INT_CONS_HILO) {
             for (int q = 0; q < 4; ++q)
                 c[q] = (double)((const float *)st)[s + q * v.plane] + (double)((const float *)lo)[s + q * v.plane];
         } else {

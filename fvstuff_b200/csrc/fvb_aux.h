@@ -20,7 +20,7 @@ struct ExtView {
 };
 
 // internal state kinds
-enum { INT_PRIM64 = 0, INT_PRIM32 = 1, INT_CONS_HILO = 2 };
+enum { INT_PRIM64 = 0, INT_PRIM32 = 1, INT_CONS_HILO = 2, INT_CONS64 = 3 };
 
 template <class R>
 cudaError_t bc_fill(R *buf, const BufView &v, int bcx, int bcy, cudaStream_t s);

@@ -29,14 +29,10 @@ void case_defaults(fvb_case *c, int kind, double x0, double y0, double L);
 // tile variant for a grid size (fvb_tune.cpp)
 int autotune_shape(int prec, int order, int n);
 
-// KEEP flux family (fvb_keep.cpp), reached through the same fvb_solver handle
-fvb_status keep_create(const fvb_config *cfg, fvb_solver **out);
-void keep_destroy(fvb_solver *s);
-fvb_status keep_init_case(fvb_solver *s, const fvb_case *c);
-fvb_status keep_set_state(fvb_solver *s, const void *src, int layout, int dtype, int where, int interior_only);
-fvb_status keep_get_state(fvb_solver *s, void *dst, int layout, int dtype, int where, int interior_only);
-fvb_status keep_step(fvb_solver *s, int nsteps, double t_stop);
-fvb_status keep_sync(fvb_solver *s, fvb_stats *st);
-fvb_status keep_stats_sums(fvb_solver *s, fvb_stats *st);
+// KEEP flux family (fvb_keep.cu): tiles of a grid, one stage (entropy-
+// distance pass + fused stage kernel), and the wave-speed max of a state
+void keep_tiles(int n, int &tiles_x, int &tiles);
+cudaError_t keep_launch_stage(const GridDev &gd, int stage, int tiles, cudaStream_t s);
+cudaError_t keep_lam_into(const GridDev &gd, cudaStream_t s);
 
 }  // namespace fvb

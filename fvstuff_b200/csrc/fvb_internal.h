@@ -30,6 +30,7 @@ struct Ctrl {
     int status;                 // fvb_status of the step control
     int clamped;                // dt was clamped to land on t_stop
     int pad;
+    unsigned long long aux;     // KEEP: bit pattern of the entropy-distance max of the stage input
 };
 
 // Device view of one grid.  Element (q, jp, ip) of a padded buffer, padded

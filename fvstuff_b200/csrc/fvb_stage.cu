@@ -19,167 +19,9 @@
 
 #include "fvb_internal.h"
 #include "fvb_physics.cuh"
+#include "fvb_device.cuh"
 
 namespace fvb {
-
-template <int PREC> struct PrecT;
-template <> struct PrecT<P64> { using R = double; using RR = double; };
-template <> struct PrecT<P32> { using R = float; using RR = double; };
-template <> struct PrecT<P32C> { using R = float; using RR = float; };
-
-__device__ __forceinline__ long long gidx(const GridDev &gd, int q, int j, int i)
-{
-    // interior coordinates (j, i), negative or >= n inside the ghost ring
-    return (long long)q * gd.plane + (long long)(j + gd.g) * gd.pitch + (i + gd.g) + gd.xoff;
-}
-
-// Coordinates of cell i and of every ghost cell that mirrors it along one
-// axis; flip marks reflected images (normal momentum negated).
-__device__ __forceinline__ int mirror_images(int i, int n, int g, int bc, int *pos, bool *flip)
-{
-    int k = 0;
-    pos[k] = i; flip[k++] = false;
-    if (bc == FVB_BC_REFLECT) {
-        if (i < g) { pos[k] = -1 - i; flip[k++] = true; }
-        if (i >= n - g) { pos[k] = 2 * n - 1 - i; flip[k++] = true; }
-    } else if (bc == FVB_BC_PERIODIC) {
-        if (i < g) { pos[k] = i + n; flip[k++] = false; }
-        if (i >= n - g) { pos[k] = i - n; flip[k++] = false; }
-    } else {
-        if (i == 0) for (int m = 1; m <= g; ++m) { pos[k] = -m; flip[k++] = false; }
-        if (i == n - 1) for (int m = 0; m < g; ++m) { pos[k] = n + m; flip[k++] = false; }
-    }
-    return k;
-}
-
-// Store a cell value into the interior and all its ghost images.
-template <class R>
-__device__ __forceinline__ void put_cell(const GridDev &gd, R *buf, int j, int i, const R v[4])
-{
-    long long c = gidx(gd, 0, j, i);
-    buf[c] = v[0];
-    buf[c + gd.plane] = v[1];
-    buf[c + 2 * gd.plane] = v[2];
-    buf[c + 3 * gd.plane] = v[3];
-    const int g = gd.g, n = gd.n;
-    if (i >= g && i < n - g && j >= g && j < n - g) return;
-    int xs[12], ys[12];
-    bool fx[12], fy[12];
-    int nx = mirror_images(i, n, g, gd.bcx, xs, fx);
-    int ny = mirror_images(j, n, g, gd.bcy, ys, fy);
-    for (int a = 0; a < ny; ++a)
-        for (int b = 0; b < nx; ++b) {
-            if (a == 0 && b == 0) continue;
-            long long e = gidx(gd, 0, ys[a], xs[b]);
-            buf[e] = v[0];
-            buf[e + gd.plane] = fx[b] ? -v[1] : v[1];
-            buf[e + 2 * gd.plane] = fy[a] ? -v[2] : v[2];
-            buf[e + 3 * gd.plane] = v[3];
-        }
-}
-
-// Error-free sum of a double-float (hi, lo) and a float increment d
-// (Knuth TwoSum for hi + d, then Dekker FastTwoSum to renormalise).
-__device__ __forceinline__ void df_add(float &hi, float &lo, float d)
-{
-    float s = __fadd_rn(hi, d);
-    float bb = __fsub_rn(s, hi);
-    float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(d, bb));
-    float l = __fadd_rn(lo, err);
-    float h2 = __fadd_rn(s, l);
-    lo = __fsub_rn(l, __fsub_rn(h2, s));
-    hi = h2;
-}
-
-// does any grid of this launch load through TMA (a single-grid launch
-// decides by its descriptor; batched grids all carry descriptors)
-__device__ __forceinline__ bool gd_has_tma(const StageArgs &a)
-{
-    return a.grids != nullptr || a.grid.tmap != nullptr;
-}
-
-struct TileCtl {
-    double dt;
-    int run;    // compute the stage on this tile
-    int copy;   // F32C stage 3 of a skipped step: carry the state across
-};
-
-// Step control, evaluated by thread 0 of each CTA for its tile's grid.
-template <int PREC>
-__device__ TileCtl tile_control(Ctrl *c, int stage, bool leader)
-{
-    TileCtl s{0.0, 0, 0};
-    if (stage == 0) { s.run = 1; return s; }
-    if (stage == 1) {
-        double t = c->t, ts = c->t_stop;
-        if (c->status != 0 || !(t < ts)) {
-            if (leader) c->active = 0;
-            return s;
-        }
-        double lam = __longlong_as_double((long long)c->lam_acc);
-        if (!(lam > 0.0)) {
-            if (leader) { c->status = FVB_ERR_BLOWUP; c->active = 0; }
-            return s;
-        }
-        double dt;
-        int clamped = 0;
-        if (PREC == P64) {
-            dt = c->cfl * c->h / lam;
-            if (t + dt > ts) { dt = ts - t; clamped = 1; }
-            if (dt < 1e-14) {
-                if (leader) { c->status = FVB_ERR_DT_UNDERFLOW; c->active = 0; }
-                return s;
-            }
-        } else if (PREC == P32) {
-            // float time and dt, as the shipped solver keeps them
-            float tf = (float)t, tsf = (float)ts;
-            float d = (float)c->cfl * (float)c->h / (float)lam;
-            if (tf + d > tsf) { d = tsf - tf; clamped = 1; }
-            if (d < 1e-14f) {
-                if (leader) { c->status = FVB_ERR_DT_UNDERFLOW; c->active = 0; }
-                return s;
-            }
-            dt = d;
-        } else {
-            // FP32 dt, FP64 accumulated time landing exactly on t_stop
-            float d = (float)(c->cfl * c->h) / (float)lam;
-            if (t + (double)d > ts) { d = (float)(ts - t); clamped = 1; }
-            if (d < 1e-14f) {
-                if (leader) { c->status = FVB_ERR_DT_UNDERFLOW; c->active = 0; }
-                return s;
-            }
-            dt = d;
-        }
-        if (leader) {
-            c->dt = dt;
-            c->active = 1;
-            c->clamped = clamped;
-            c->lam_cur = c->lam_acc;
-        }
-        s.dt = dt;
-        s.run = 1;
-        return s;
-    }
-    if (!c->active) {
-        s.copy = (stage == 3 && PREC == P32C);
-        return s;
-    }
-    s.dt = c->dt;
-    s.run = 1;
-    if (stage == 2 && leader) c->lam_acc = 0ull;
-    return s;
-}
-
-template <int PREC>
-__device__ __forceinline__ void leader_finish(Ctrl *c)
-{
-    double t = c->t, dt = c->dt;
-    if (PREC == P32) t = (double)((float)t + (float)dt);
-    else if (PREC == P32C) t = c->clamped ? c->t_stop : t + dt;
-    else t = t + dt;
-    c->t = t;
-    c->step = c->step + 1;
-}
 
 // ---------------------------------------------------------------------------
 // TMA and mbarrier primitives (sm_90+ PTX; no cluster multicast anywhere)
@@ -265,8 +107,57 @@ __device__ __forceinline__ void issue_tile_load(const GridDev &gd, int stage, in
     }
 }
 
+// Flux through one face of the working tile W ([6][SH][SW]: rho, u, v, p,
+// c, E) whose right/top cell is at `base`; XDIR: x-face (normal u), else
+// y-face (normal v).  Writes the 4 Cartesian components to out[q * ostride].
+template <int PREC, int ORDER, int SW, int PL, bool XDIR, class R>
+__device__ __forceinline__ void face_one(const R *W, int base, R *out, int ostride, const GasF<R> &gf,
+                                         const Gas<R> &gs)
+{
+    using RR = typename PrecT<PREC>::RR;
+    constexpr int G = (ORDER + 1) / 2;
+    constexpr int ST = XDIR ? 1 : SW;
+    constexpr int QN = XDIR ? 1 : 2, QT = XDIR ? 2 : 1;
+    constexpr int QS[4] = {0, QN, QT, 3};
+    R L[4], Rv[4], WL[4], WR[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const R *v = W + QS[m] * PL + base;
+        R s[2 * G];
+#pragma unroll
+        for (int d = 0; d < 2 * G; ++d) s[d] = v[(d - G) * ST];
+        if constexpr (PREC != P32) upface_fast<R, ORDER>(s, L[m], Rv[m]);
+        else upface<R, RR, ORDER>(s, L[m], Rv[m]);
+        WL[m] = s[G - 1];
+        WR[m] = s[G];
+    }
+    L[0] = floor14(L[0]); Rv[0] = floor14(Rv[0]);
+    L[3] = floor14(L[3]); Rv[3] = floor14(Rv[3]);
+    R Fn[4];
+    if constexpr (PREC != P32) {
+        const R *CE = W + 4 * PL + base;
+        face_flux_fast<R>(L, Rv, WL, WR, CE[-ST], CE[0], CE[PL - ST], CE[PL], gf, Fn);
+    } else {
+        R Fh[4], Fl[4];
+        hllc<R>(L, Rv, Fh, gs);
+        hlle<R>(WL, WR, Fl, gs);
+        const R sd = ducros<R>(WL[3], WR[3]);
+        const R one_m = R(1) - sd;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) Fn[q] = one_m * Fh[q] + sd * Fl[q];
+    }
+    out[0] = Fn[0];
+    out[ostride] = Fn[QN];
+    out[2 * ostride] = Fn[QT];
+    out[3 * ostride] = Fn[3];
+}
+
+// resident CTAs per SM the kernel is compiled for: three for FP32c (its
+// tile fits 3 x 68 KB of shared memory), two otherwise
+template <int PREC> struct MinBlocks { static constexpr int v = PREC == P32C ? 3 : 2; };
+
 template <int PREC, int ORDER, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, 1) stage_kernel(const __grid_constant__ StageArgs a)
+__global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __grid_constant__ StageArgs a)
 {
     using R = typename PrecT<PREC>::R;
     using RR = typename PrecT<PREC>::RR;
@@ -404,49 +295,16 @@ __global__ void __launch_bounds__(NT, 1) stage_kernel(const __grid_constant__ St
         const R dt = R(ctl.dt);
         const R inv_h = R(1.0 / gd.h);
 
-        // ---- 3. face fluxes -------------------------------------------------
-        for (int f = tid; f < NXF + NYF; f += NT) {
-            const bool xf = f < NXF;
-            int r, c, st;
-            if (xf) { r = f / (TX + 1); c = f - r * (TX + 1); st = 1; }
-            else { int f2 = f - NXF; r = f2 / TX; c = f2 - r * TX; st = SW; }
-            const int base = (r + G) * SW + (c + G);  // cell on the right/top of the face
-            const int qn = xf ? 1 : 2, qt = xf ? 2 : 1;
-            const int qs[4] = {0, qn, qt, 3};
-            R L[4], Rv[4], WL[4], WR[4];
-#pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                const R *v = W + qs[m] * PL + base;
-                R s[2 * G];
-#pragma unroll
-                for (int d = 0; d < 2 * G; ++d) s[d] = v[(d - G) * st];
-                if constexpr (FAST) upface_fast<R, ORDER>(s, L[m], Rv[m]);
-                else upface<R, RR, ORDER>(s, L[m], Rv[m]);
-                WL[m] = s[G - 1];
-                WR[m] = s[G];
-            }
-            L[0] = floor14(L[0]); Rv[0] = floor14(Rv[0]);
-            L[3] = floor14(L[3]); Rv[3] = floor14(Rv[3]);
-            R Fn[4];
-            if constexpr (FAST) {
-                const R *CE = W + 4 * PL + base;
-                face_flux_fast<R>(L, Rv, WL, WR, CE[-st], CE[0], CE[PL - st], CE[PL], gf, Fn);
-            } else {
-                R Fh[4], Fl[4];
-                hllc<R>(L, Rv, Fh, gs);
-                hlle<R>(WL, WR, Fl, gs);
-                const R sd = ducros<R>(WL[3], WR[3]);
-                const R one_m = R(1) - sd;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) Fn[q] = one_m * Fh[q] + sd * Fl[q];
-            }
-            if (xf) {
-                R *o = FX + r * (TX + 1) + c;
-                o[0] = Fn[0]; o[TY * (TX + 1)] = Fn[1]; o[2 * TY * (TX + 1)] = Fn[2]; o[3 * TY * (TX + 1)] = Fn[3];
-            } else {
-                R *o = FY + r * TX + c;
-                o[0] = Fn[0]; o[(TY + 1) * TX] = Fn[2]; o[2 * (TY + 1) * TX] = Fn[1]; o[3 * (TY + 1) * TX] = Fn[3];
-            }
+        // ---- 3. face fluxes: x-faces, then y-faces (compile-time strides) ---
+        for (int f = tid; f < NXF; f += NT) {
+            const int r = f / (TX + 1), c = f - r * (TX + 1);
+            face_one<PREC, ORDER, SW, PL, true>(W, (r + G) * SW + (c + G), FX + r * (TX + 1) + c, TY * (TX + 1),
+                                               gf, gs);
+        }
+        for (int f = tid; f < NYF; f += NT) {
+            const int r = f / TX, c = f - r * TX;
+            face_one<PREC, ORDER, SW, PL, false>(W, (r + G) * SW + (c + G), FY + r * TX + c, (TY + 1) * TX, gf,
+                                                gs);
         }
         __syncthreads();
 

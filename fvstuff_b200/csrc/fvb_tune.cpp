@@ -1,14 +1,143 @@
-// fvb_tune.cpp -- choice of the stage-kernel tile variant.
+// fvb_tune.cpp -- choice of the stage-kernel tile variant (halo-tile shape
+// and threads per tile) by measurement.
+//
+// On first use for a (device, precision, order, grid-size class) the tuner
+// builds a scratch grid of a representative size (the grid's own size, at
+// most 1024^2), fills it with a smooth state, and times a few SSP-RK3 steps
+// of every tile variant that can be resident on the device with CUDA
+// events; the fastest wins and is cached for the process.  FVB_TILE=<k>
+// forces variant k; FVB_AUTOTUNE=0 selects variant 0 without measuring.
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "fvb_host.h"
 
 namespace fvb {
+namespace {
+
+std::mutex g_mu;
+std::map<std::tuple<int, int, int, int>, int> g_cache;
+
+int size_class(int n)
+{
+    int c = 0;
+    for (int m = 64; m < n && c < 5; m *= 2) ++c;  // <=64, <=128, <=256, <=512, <=1024, larger
+    return c;
+}
+
+// time `steps` steps of variant `shape` on a scratch grid; < 0 on failure
+float time_shape(int prec, int order, int n, int shape, cudaStream_t s)
+{
+    const int g = (order + 1) / 2;
+    Geometry G = make_geometry(n, g, prec == P64 ? FVB_PREC_F64 : prec == P32 ? FVB_PREC_F32 : FVB_PREC_F32C);
+    const size_t ctrl_off = (G.bytes + 255) / 256 * 256, map_off = ctrl_off + 256;
+    const size_t stage_bytes = (size_t)4 * n * n * sizeof(double);
+    void *block = nullptr, *stage = nullptr;
+    if (cudaMalloc(&block, map_off + TM_COUNT * sizeof(CUtensorMap)) != cudaSuccess) return -1.f;
+    if (cudaMalloc(&stage, stage_bytes) != cudaSuccess) { cudaFree(block); return -1.f; }
+    float ms = -1.f;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    do {
+        GridDev gd{};
+        grid_pointers(gd, block, G, prec == P64 ? FVB_PREC_F64 : prec == P32 ? FVB_PREC_F32 : FVB_PREC_F32C);
+        gd.bcx = gd.bcy = FVB_BC_PERIODIC;
+        gd.h = 1.0 / n;
+        gd.gam = 1.4;
+        gd.ctrl = (Ctrl *)((char *)block + ctrl_off);
+        int tiles;
+        tile_dims(shape, n, gd.tiles_x, tiles);
+        CUtensorMap maps[TM_COUNT];
+        gd.tmap = nullptr;
+        if (encode_tile_maps(gd, prec, order, shape, maps)) {
+            CUtensorMap *dm = (CUtensorMap *)((char *)block + map_off);
+            if (cudaMemcpy(dm, maps, sizeof maps, cudaMemcpyHostToDevice) != cudaSuccess) break;
+            gd.tmap = dm;
+        }
+        fvb_case c;
+        case_defaults(&c, FVB_CASE_KH, 0.0, 0.0, 1.0);
+        const int internal = prec_internal(prec == P64 ? FVB_PREC_F64 : prec == P32 ? FVB_PREC_F32 : FVB_PREC_F32C);
+        ExtView ev{1, g, n + 2 * g, FVB_LAYOUT_PRIM, FVB_F64};
+        BufView v = view_of(gd);
+        if (cudaMemsetAsync(block, 0, G.bytes, s) != cudaSuccess) break;
+        if (init_case_prim64((double *)stage, n, 0.0, 0.0, gd.h, 1.4, c, s) != cudaSuccess) break;
+        if (import_state(stage, ev, gd.st[0], gd.lo[0], v, internal, 1.4, s) != cudaSuccess) break;
+        cudaError_t e = internal == INT_PRIM64 ? bc_fill<double>((double *)gd.st[0], v, 1, 1, s)
+                                               : bc_fill<float>((float *)gd.st[0], v, 1, 1, s);
+        if (e == cudaSuccess && internal == INT_CONS_HILO) e = bc_fill<float>((float *)gd.lo[0], v, 1, 1, s);
+        if (e == cudaSuccess) e = lam_into(gd.st[0], v, internal, 1.4, &gd.ctrl->lam_acc, s);
+        if (e == cudaSuccess) e = ctrl_set(gd.ctrl, 1e300, 1, 0.0, 0.4, gd.h, s);
+        if (e != cudaSuccess) break;
+        int per_sm = stage_max_ctas_per_sm(prec, order, shape), sms = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (per_sm <= 0) break;
+        const int ctas = tiles < per_sm * sms ? tiles : per_sm * sms;
+        StageArgs a{};
+        a.grid = gd;
+        a.ntiles_static = tiles;
+        auto run = [&](int steps) {
+            int parity = 0;
+            for (int k = 0; k < steps; ++k) {
+                for (int stage = 1; stage <= 3; ++stage) {
+                    a.stage = stage;
+                    a.parity = parity;
+                    if (launch_stage(prec, order, shape, a, ctas, s) != cudaSuccess) return false;
+                }
+                if (prec == P32C) parity ^= 1;
+            }
+            return true;
+        };
+        if (!run(2)) break;  // warm-up (even: F32C ends on its start buffer)
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, s);
+        if (!run(4)) break;
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) break;
+        cudaEventElapsedTime(&ms, e0, e1);
+    } while (0);
+    cudaStreamSynchronize(s);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(stage);
+    cudaFree(block);
+    cudaGetLastError();  // a failed variant must not poison later calls
+    return ms;
+}
+
+}  // namespace
 
 int autotune_shape(int prec, int order, int n)
 {
-    (void)prec;
-    (void)order;
-    (void)n;
-    return 0;
+    if (const char *f = std::getenv("FVB_TILE")) {
+        int k = std::atoi(f);
+        if (k >= 0 && k < kNumTileShapes) return k;
+    }
+    if (const char *a = std::getenv("FVB_AUTOTUNE"))
+        if (a[0] == '0') return 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(dev, prec, order, size_class(n));
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_cache.find(key);
+    if (it != g_cache.end()) return it->second;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return 0;
+    const int nt = n < 1024 ? (n < 16 ? 16 : n) : 1024;
+    int best = 0;
+    float best_ms = -1.f;
+    for (int shape = 0; shape < kNumTileShapes; ++shape) {
+        float ms = time_shape(prec, order, nt, shape, s);
+        if (ms > 0 && (best_ms < 0 || ms < best_ms)) {
+            best_ms = ms;
+            best = shape;
+        }
+    }
+    cudaStreamDestroy(s);
+    g_cache[key] = best;
+    return best;
 }
 
 }  // namespace fvb

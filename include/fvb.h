@@ -147,6 +147,14 @@ FVB_API fvb_status fvb_get_state(fvb_solver *s, void *dst, int layout, int dtype
 /* hi/lo words of the compensated state, conserved, interior, FP32 each */
 FVB_API fvb_status fvb_get_state_hilo(fvb_solver *s, float *hi, float *lo);
 
+/* Checkpoint / resume: the exact internal state (every padded buffer word),
+ * the time, the step count and the wave-speed max that sets the next dt, so
+ * a resumed run continues bit for bit.  The reference writes images only
+ * (fv_up7_ducros_2d.cu:757-881) and cannot resume.  load requires a solver
+ * created with the same n, flux, order and precision. */
+FVB_API fvb_status fvb_save(fvb_solver *s, const char *path);
+FVB_API fvb_status fvb_load(fvb_solver *s, const char *path);
+
 /* Enqueue up to nsteps SSP-RK3 steps on the solver's stream without waiting.
  * Each step picks dt = cfl h / lam_max, clamped so t lands on t_stop; steps
  * at t >= t_stop do nothing.  Replaces the loop body of

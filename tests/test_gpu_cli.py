@@ -1,0 +1,110 @@
+"""Command-line drop-ins and outputs on the GPU: fvb_up7 (fv_up7's CLI,
+composite PPM frames, raw .bin frames, frame 99 on blow-up) and fvb_keep
+(keep_fv's CLI, 2-panel PNG), and exact checkpoint / resume."""
+from __future__ import annotations
+
+import struct
+import subprocess
+import zlib
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import fvstuff_b200 as F
+from cases import riemann4
+
+pytestmark = pytest.mark.gpu
+BIN = Path(F.__file__).resolve().parent / "bin"
+
+
+def _ppm(path):
+    data = path.read_bytes()
+    parts = data.split(b"\n", 3)
+    assert parts[0] == b"P6" and parts[2] == b"255"
+    w, h = map(int, parts[1].split())
+    assert len(parts[3]) == 3 * w * h
+    return w, h, np.frombuffer(parts[3], np.uint8).reshape(h, w, 3)
+
+
+def _png(path):
+    data = path.read_bytes()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat, w = 8, b"", None
+    while pos < len(data):
+        ln, typ = struct.unpack(">I4s", data[pos:pos + 8])
+        body = data[pos + 8:pos + 8 + ln]
+        crc, = struct.unpack(">I", data[pos + 8 + ln:pos + 12 + ln])
+        assert crc == zlib.crc32(typ + body) & 0xFFFFFFFF
+        if typ == b"IHDR":
+            w, h = struct.unpack(">II", body[:8])
+        if typ == b"IDAT":
+            idat += body
+        pos += 12 + ln
+    raw = zlib.decompress(idat)
+    assert len(raw) == h * (3 * w + 1)
+    return w, h
+
+
+def test_fvb_up7_frames(tmp_path):
+    r = subprocess.run([str(BIN / "fvb_up7"), "48", "--t-end", "0.02", "--frames", "2", "--bin"], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert "Done:" in r.stdout and "frame  2/2" in r.stdout
+    for k in range(3):
+        w, h, img = _ppm(tmp_path / ("sod_%04d.ppm" % k))
+        assert (w, h) == (96, 96)
+        raw = (tmp_path / ("sod_%04d.bin" % k)).read_bytes()
+        n, = struct.unpack("<i", raw[:4])
+        assert n == 48 and len(raw) == 4 + 2 * 4 * n * n
+        rho = np.frombuffer(raw[4:4 + 4 * n * n], np.float32).reshape(n, n)
+        assert 0.1 < rho.min() and rho.max() < 11.5
+    # the density panel of the initial frame is symmetric under y -> -y
+    # (circular Sod), to within one colour level
+    _, _, img0 = _ppm(tmp_path / "sod_0000.ppm")
+    panel = img0[:48, :48].astype(int)
+    assert np.max(np.abs(panel - panel[::-1, :])) <= 1
+
+
+def test_fvb_up7_resume_matches_straight_run(tmp_path):
+    args = [str(BIN / "fvb_up7"), "32", "--case", "vortex", "--t-end", "0.4", "--frames", "2", "--no-ppm", "--bin"]
+    subprocess.run(args + ["--save", "full.ckpt"], cwd=tmp_path, check=True, capture_output=True, timeout=120)
+    half = [str(BIN / "fvb_up7"), "32", "--case", "vortex", "--t-end", "0.2", "--frames", "1", "--no-ppm",
+            "--save", "half.ckpt"]
+    subprocess.run(half, cwd=tmp_path, check=True, capture_output=True, timeout=120)
+    s1 = F.Solver(32, bc="periodic", x0=-5, y0=-5, length=10.0)
+    s1.load(tmp_path / "full.ckpt")
+    s2 = F.Solver(32, bc="periodic", x0=-5, y0=-5, length=10.0)
+    s2.load(tmp_path / "half.ckpt")
+    assert s2.sync().t == pytest.approx(0.2, abs=1e-15)
+    s2.advance(0.4)
+    assert s2.sync().t == s1.sync().t
+    # frame-clamped stepping differs between the two runs only in where the
+    # stops fall; both land on 0.4 through the same schedule of stops here
+    assert np.array_equal(s1.get_state(), s2.get_state())
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32c"])
+def test_checkpoint_resume_is_exact(tmp_path, prec):
+    n = 40
+    a = F.Solver(n, bc="transmissive", precision=prec, cfl=0.5)
+    a.set_state(riemann4(n, seed=3), interior=True)
+    a.step(7)
+    a.save(tmp_path / "c.ckpt")
+    a.step(9)
+    b = F.Solver(n, bc="transmissive", precision=prec, cfl=0.5)
+    b.load(tmp_path / "c.ckpt")
+    assert b.sync().steps == 7
+    b.step(9)
+    assert b.sync().t == a.sync().t
+    assert np.array_equal(a.get_state(layout="cons", interior=True), b.get_state(layout="cons", interior=True))
+
+
+def test_fvb_keep_lmv(tmp_path):
+    r = subprocess.run([str(BIN / "fvb_keep"), "40", "lmv", "0.1", "--t-end", "0.05"], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert "FINAL L2 ERRORS" in r.stdout
+    for k in range(11):
+        w, h = _png(tmp_path / "figures" / ("keep_lmv_%04d.png" % k))
+        assert (w, h) == (80, 40)

@@ -112,6 +112,22 @@ def test_oracle_matches_reference_host_t_stop():
     assert np.array_equal(U, V)
 
 
+def test_keep_reference_scheme_loses_energy_on_sod():
+    """A property of the reference scheme the GPU path reproduces: on the
+    circular Sod case the rk_stage floor E >= 1e-14 (keep_fv_euler_2d.cu:
+    390-391) clips energies the scheme drives negative, so total energy
+    drifts while mass and momentum stay conserved."""
+    n, h = 48, 1.0 / 48
+    U = O.keep_ic(n, h, False)
+    O.bc(U, n, 2, 1)
+    sums = lambda V: [V[q, 2:2 + n, 2:2 + n].sum() * h * h for q in range(4)]
+    a = sums(U)
+    O.keep_run(U, n, h, 0.2, 5)
+    b = sums(U)
+    assert abs(b[0] - a[0]) < 1e-14 and abs(b[1] - a[1]) < 1e-14 and abs(b[2] - a[2]) < 1e-14
+    assert b[3] - a[3] > 1e-6
+
+
 @needs_ref
 def test_keep_oracle_matches_reference_host():
     n = 20
