@@ -176,7 +176,6 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
     R *W = IN + NIN * PL;
     R *FX = W + 6 * PL;               // [4][TY][TX+1]
     R *FY = FX + 4 * TY * (TX + 1);   // [4][TY+1][TX]
-    __shared__ TileCtl s_ctl;
     __shared__ double s_red[NW];
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ int s_err;
@@ -201,26 +200,37 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
         return a.grid;
     };
 
+    // every thread waits on the mbarrier itself (the completed phase makes the
+    // TMA bytes visible to it); the barrier after the wait only agrees on s_err
     uint32_t phase = 0;
+    auto wait_box = [&](bool tma) {
+        if (tma) {
+            if (mbar_wait(&s_bar, phase)) phase ^= 1;
+            else s_err = 1;
+        }
+        __syncthreads();
+    };
     int t = blockIdx.x;
-    if (t < ntiles) {
-        int tile;
-        GridDev g0 = grid_of(t, tile);
-        issue_tile_load<PREC, G, SW, SH, NT>(g0, a.stage, cur, tile, IN, &s_bar, tid);
+    {
+        bool tma = false;
+        if (t < ntiles) {
+            int tile;
+            GridDev g0 = grid_of(t, tile);
+            issue_tile_load<PREC, G, SW, SH, NT>(g0, a.stage, cur, tile, IN, &s_bar, tid);
+            tma = g0.tmap != nullptr;
+        }
+        wait_box(tma);
     }
+    // single grid: the stage-3 wave-speed max is reduced once per CTA
+    double lacc = 0.0;
     for (; t < ntiles; t += gridDim.x) {
         int tile;
         const GridDev gd = grid_of(t, tile);
         const int n = gd.n;
         const int tx0 = (tile % gd.tiles_x) * TX, ty0 = (tile / gd.tiles_x) * TY;
-        if (tid == 0) s_ctl = tile_control<PREC>(gd.ctrl, a.stage, tile == 0);
-        // ---- 1. wait for this tile's halo box; convert into W --------------
-        if (gd.tmap) {
-            if (mbar_wait(&s_bar, phase)) phase ^= 1;
-            else s_err = 1;
-        }
-        __syncthreads();
-        const TileCtl ctl = s_ctl;
+        // ---- 1. the tile's halo box has landed in IN; convert into W --------
+        // (the step control is read by every thread: only the leader writes)
+        const TileCtl ctl = tile_control<PREC>(gd.ctrl, a.stage, tid == 0 && tile == 0);
         const Gas<R> gs{R(gd.gam), R(gd.gam) - R(1)};
         const GasF<R> gf{R(gd.gam), R(1.0 / (gd.gam - 1.0)), R(gd.gam) - R(1)};
         if (s_err) {
@@ -231,6 +241,12 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
         if (ctl.run && a.stage >= 0) {
             for (int k = tid; k < PL; k += NT) {
                 R w0 = IN[k], w1 = IN[PL + k], w2 = IN[2 * PL + k], w3 = IN[3 * PL + k];
+                // sound speed and energy only where the HLLE reads them: the
+                // interior rows x columns [G-1, G+TX], and rows G-1 and G+TY
+                // x the interior columns
+                const int r = k / SW, c = k - r * SW;
+                const bool ce = ((unsigned)(r - G) < (unsigned)TY && (unsigned)(c - (G - 1)) < (unsigned)(TX + 2)) ||
+                                ((r == G - 1 || r == G + TY) && (unsigned)(c - G) < (unsigned)TX);
                 if constexpr (PREC == P32C) {
                     if (a.stage >= 2) {
                         w0 += IN[4 * PL + k]; w1 += IN[5 * PL + k]; w2 += IN[6 * PL + k]; w3 += IN[7 * PL + k];
@@ -240,13 +256,25 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
                     w1 *= ir;
                     w2 *= ir;
                     w3 = gf.gm1 * (E - 0.5f * w0 * (w1 * w1 + w2 * w2));
-                    W[5 * PL + k] = E;
+                    if (ce) {
+                        const float cs2 = gf.gam * w3 * ir;
+                        W[4 * PL + k] = fsqrt(cs2 > 1e-14f ? cs2 : 1e-14f);
+                        W[5 * PL + k] = E;
+                    }
+                } else if constexpr (FAST) {
+                    if (ce) {
+                        R cc, ee;
+                        cell_ce<R>(w0, w1, w2, w3, gf, cc, ee);
+                        W[4 * PL + k] = cc;
+                        W[5 * PL + k] = ee;
+                    }
                 }
                 W[k] = w0; W[PL + k] = w1; W[2 * PL + k] = w2; W[3 * PL + k] = w3;
             }
         }
         __syncthreads();
         // ---- 2. load the next tile into IN (asynchronous through TMA) -------
+        bool next_tma = false;
         {
             const int tn = t + gridDim.x;
             if (tn < ntiles) {
@@ -255,6 +283,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
                 // order this CTA's reads of IN before the async-proxy writes
                 if (tid == 0 && gn.tmap) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 issue_tile_load<PREC, G, SW, SH, NT>(gn, a.stage, cur, tilen, IN, &s_bar, tid);
+                next_tma = gn.tmap != nullptr;
             }
         }
 
@@ -272,25 +301,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
                     put_cell<float>(gd, (float *)gd.lo[nxt], j, i, vl);
                 }
             }
-            __syncthreads();
+            wait_box(next_tma);
             continue;
-        }
-        // sound speed and energy of the cells the HLLE uses: the cross of
-        // the interior rows x [G-1, G+TX] and the interior columns x {G-1, G+TY}
-        if constexpr (FAST) {
-            constexpr int NA = TY * (TX + 2), NB = 2 * TX;
-            for (int k = tid; k < NA + NB; k += NT) {
-                int r, c;
-                if (k < NA) { r = G + k / (TX + 2); c = G - 1 + k % (TX + 2); }
-                else { int m = k - NA; r = (m < TX) ? G - 1 : G + TY; c = G + (m % TX); }
-                const int e = r * SW + c;
-                const R rho = W[e], u = W[PL + e], v = W[2 * PL + e], p = W[3 * PL + e];
-                const R ir = frcp(rho);
-                R cs2 = gf.gam * p * ir;
-                W[4 * PL + e] = fsqrt(cs2 > FVB_LIT(R, 1e-14) ? cs2 : FVB_LIT(R, 1e-14));
-                if constexpr (PREC != P32C) W[5 * PL + e] = p * gf.igm1 + R(0.5) * rho * (u * u + v * v);
-            }
-            __syncthreads();
         }
         const R dt = R(ctl.dt);
         const R inv_h = R(1.0 / gd.h);
@@ -436,18 +448,35 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
 
         // ---- 5. max wave speed of the new state (stage 3) ------------------
         if (a.stage == 3) {
+            if (tid == 0 && tile == 0) leader_finish<PREC>(gd.ctrl);
+            if (batched) {
+                // tiles of one CTA belong to different instances: per tile
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-            if ((tid & 31) == 0) s_red[tid >> 5] = lmax;
-            __syncthreads();
-            if (tid == 0) {
-                double m = 0.0;
-                for (int w = 0; w < NW; ++w) m = fmax(m, s_red[w]);
-                atomicMax(&gd.ctrl->lam_acc, (unsigned long long)__double_as_longlong(m));
-                if (tile == 0) leader_finish<PREC>(gd.ctrl);
+                for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+                if ((tid & 31) == 0) s_red[tid >> 5] = lmax;
+                __syncthreads();
+                if (tid == 0) {
+                    double m = 0.0;
+                    for (int w = 0; w < NW; ++w) m = fmax(m, s_red[w]);
+                    atomicMax(&gd.ctrl->lam_acc, (unsigned long long)__double_as_longlong(m));
+                }
+            } else {
+                lacc = fmax(lacc, lmax);
             }
         }
+        // ---- 6. next tile's halo box: wait, then release W / FX / FY -------
+        wait_box(next_tma);
+    }
+    if (!batched && a.stage == 3) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lacc = fmax(lacc, __shfl_xor_sync(0xffffffffu, lacc, o));
+        if ((tid & 31) == 0) s_red[tid >> 5] = lacc;
         __syncthreads();
+        if (tid == 0 && a.grid.ctrl) {
+            double m = 0.0;
+            for (int w = 0; w < NW; ++w) m = fmax(m, s_red[w]);
+            if (m > 0.0) atomicMax(&a.grid.ctrl->lam_acc, (unsigned long long)__double_as_longlong(m));
+        }
     }
     // a load still in flight after an error: wait for it (bounded) so no
     // copy into this CTA's shared memory outlives it

@@ -11,8 +11,12 @@ Conditioning of the reference scheme sets the bars:
   steps) and amplifies last-bit differences; parity is held at 1e-12 over the
   first two steps;
 * low-Mach vortex: the energy flux divides by (dV3^2 + 1e-16) with dV3 small,
-  so the reference's own GPU and host builds differ at ~3e-12 per step; ours
-  must stay within ten times that spread (and below 1e-10).
+  so the reference's own GPU and host builds differ at ~3e-12 per step (4e-10
+  after 10 steps at 16^2); ours must stay within ten times that spread.  The
+  vortex is chaotic under last-bit perturbation: a 2e-16 relative
+  perturbation of the initial state moves the oracle's L2 errors by 3e-10 at
+  t = 0.01 (69 steps at 64^2) but by 1e-3 at t = 0.05 (342 steps), so the
+  L2-error check runs to t = 0.01.
 """
 from __future__ import annotations
 
@@ -64,12 +68,12 @@ def test_keep_lmv_matches_oracle_within_reference_spread(n):
     status, t, k, lmax, dt = O.keep_run(ref, n, h, 0.2, steps)
     assert status == 0 and st.status == 0 and st.steps == k == steps
     err = rel_linf(_interior(s.get_state(layout="cons"), n), _interior(ref, n))
-    bar = 1e-10
+    bar = 1e-9
     if O.have_ref_gpu():
         g = U.copy()
         O.refg_keep_run(g, n, h, 0.2, steps)
         spread = rel_linf(_interior(g, n), _interior(ref, n))
-        bar = min(bar, max(1e-12, 10 * spread))
+        bar = max(1e-12, 10 * spread)
         print("KEEP lmv %d^2 x %d: ours vs oracle %.2e, reference GPU vs oracle %.2e" % (n, steps, err, spread))
     assert err <= bar
     assert abs(st.t - t) <= 1e-11 * t
@@ -101,8 +105,8 @@ def test_keep_device_initial_state_and_lmv_error():
     ref = O.keep_ic(n, h, True)
     assert rel_linf(_interior(s.get_state(layout="cons"), n), _interior(ref, n)) <= 1e-13
     # the L2 errors against the exact stationary vortex (keep_fv_euler_2d.cu:
-    # 516-536) after the same run agree with the oracle's
-    t_end = 0.05
+    # 516-536) after the same 69-step run agree with the oracle's
+    t_end = 0.01
     st = s.advance(t_end)
     O.bc(ref, n, 2, 1)
     O.keep_run(ref, n, h, 0.2, 10 ** 6, t_stop=t_end)
