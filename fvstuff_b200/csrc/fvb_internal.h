@@ -88,6 +88,11 @@ constexpr TileShape kTileShapes[kNumTileShapes] = {
 // tile shape into host memory; false if this grid cannot use TMA
 bool encode_tile_maps(const GridDev &gd, int prec, int order, int shape, CUtensorMap out[TM_COUNT]);
 
+// the FP32-compensated stage kernel of a tile shape and its shared memory
+// (fvb_stage32c.cu)
+void *stage32c_fn(int shape, bool batched);
+size_t stage32c_smem(int shape);
+
 // launchers (fvb_stage.cu)
 cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int grid_ctas,
                          cudaStream_t s);

@@ -17,95 +17,14 @@
 // per step, by one launch per stage and none.
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "fvb_internal.h"
 #include "fvb_physics.cuh"
 #include "fvb_device.cuh"
+#include "fvb_tma.cuh"
 
 namespace fvb {
-
-// ---------------------------------------------------------------------------
-// TMA and mbarrier primitives (sm_90+ PTX; no cluster multicast anywhere)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// one 3-D tiled tensor load global -> shared, completing on `bar`
-__device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-        "[%5];" ::"r"(smem_u32(dst)),
-        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// bounded wait for phase `parity` of `bar`; false when the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
-{
-    for (uint32_t it = 0; it < (1u << 24); ++it) {
-        uint32_t ok;
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-            : "=r"(ok)
-            : "r"(smem_u32(bar)), "r"(parity)
-            : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
-
-// The halo box of a tile in one grid: TMA when the grid has descriptors,
-// else cooperative loads by the whole CTA (the caller's IDX_P arrays).
-template <int PREC, int G, int SW, int SH, int NT, class R>
-__device__ __forceinline__ void issue_tile_load(const GridDev &gd, int stage, int parity, int tile, R *IN,
-                                                uint64_t *bar, int tid)
-{
-    constexpr int TXd = SW - 2 * G, TYd = SH - 2 * G;
-    const int tx0 = (tile % gd.tiles_x) * TXd, ty0 = (tile / gd.tiles_x) * TYd;
-    const bool two = (PREC == P32C) && (stage == 2 || stage == 3);
-    if (gd.tmap) {
-        if (tid == 0) {
-            constexpr uint32_t box = 4u * SW * SH * sizeof(R);
-            mbar_expect_tx(bar, two ? 2 * box : box);
-            int m0;
-            if (PREC == P32C) m0 = parity ? TM_ST1 : TM_ST0;
-            else m0 = stage == 2 ? TM_K1 : stage == 3 ? TM_K2 : TM_ST0;
-            const int x = gd.xoff + tx0;
-            tma_load3(IN, gd.tmap + m0, x, ty0, 0, bar);
-            if (two) tma_load3(IN + 4 * SW * SH, gd.tmap + (stage == 2 ? TM_K1 : TM_K2), x, ty0, 0, bar);
-        }
-        return;
-    }
-    const R *src = (const R *)(PREC == P32C ? gd.st[parity]
-                                            : (stage == 2 ? gd.k1 : stage == 3 ? gd.k2 : gd.st[0]));
-    const R *inc = two ? (const R *)(stage == 2 ? gd.k1 : gd.k2) : nullptr;
-    const int np = gd.n + 2 * G;
-    for (int k = tid; k < SH * SW; k += NT) {
-        int r = k / SW, c = k - r * SW;
-        int jp = ty0 + r, ip = tx0 + c;
-        bool in = jp < np && ip < np;
-        long long e = (long long)jp * gd.pitch + ip + gd.xoff;
-        for (int q = 0; q < 4; ++q) {
-            IN[q * SH * SW + k] = in ? src[e + q * gd.plane] : R(0);
-            if (two) IN[(4 + q) * SH * SW + k] = in ? inc[e + q * gd.plane] : R(0);
-        }
-    }
-}
 
 // Flux through one face of the working tile W ([6][SH][SW]: rho, u, v, p,
 // c, E) whose right/top cell is at `base`; XDIR: x-face (normal u), else
@@ -152,13 +71,12 @@ __device__ __forceinline__ void face_one(const R *W, int base, R *out, int ostri
     out[3 * ostride] = Fn[3];
 }
 
-// resident CTAs per SM the kernel is compiled for: three for FP32c (its
-// tile fits 3 x 68 KB of shared memory), two otherwise
-template <int PREC> struct MinBlocks { static constexpr int v = PREC == P32C ? 3 : 2; };
-
-template <int PREC, int ORDER, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __grid_constant__ StageArgs a)
+// The FP64 and FP32 (reference-rounding) stage kernel, two CTAs per SM; the
+// FP32-compensated form has its own kernel (fvb_stage32c.cu).
+template <int PREC, int ORDER, int TX, int TY, int NT, bool BATCHED>
+__global__ void __launch_bounds__(NT, 2) stage_kernel(const __grid_constant__ StageArgs a)
 {
+    static_assert(PREC == P64 || PREC == P32, "FP64 and FP32 primitive-state forms");
     using R = typename PrecT<PREC>::R;
     using RR = typename PrecT<PREC>::RR;
     constexpr int G = (ORDER + 1) / 2;
@@ -167,41 +85,31 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
     constexpr int NW = NT / 32;
     // the throughput paths keep each cell's sound speed and energy too
     constexpr bool FAST = (PREC != P32);
-    constexpr int NIN = PREC == P32C ? 8 : 4;  // planes of one halo box load
-
     // IN: the tile as loaded (TMA lands here); W: primitives (+ c, E) the
     // faces are computed from, so IN can take the next tile meanwhile
     extern __shared__ __align__(128) unsigned char smem_raw[];
     R *IN = reinterpret_cast<R *>(smem_raw);
-    R *W = IN + NIN * PL;
+    R *W = IN + 4 * PL;
     R *FX = W + 6 * PL;               // [4][TY][TX+1]
     R *FY = FX + 4 * TY * (TX + 1);   // [4][TY+1][TX]
     __shared__ double s_red[NW];
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ int s_err;
+    __shared__ __align__(16) TileHdr s_hdr[2];
+    __shared__ TileRef s_ref_next;  // batched: table entry of the CTA's next tile
 
     const int tid = threadIdx.x;
-    const bool batched = (a.grids != nullptr);
+    constexpr bool batched = BATCHED;
     const int ntiles = batched ? *a.ntiles : a.ntiles_static;
-    const int cur = a.parity, nxt = a.parity ^ 1;
+    const int cur = a.parity;
     if (tid == 0) {
         mbar_init(&s_bar, 1);
         s_err = 0;
     }
     __syncthreads();
 
-    auto grid_of = [&](int t, int &tile) -> GridDev {
-        if (batched) {
-            TileRef tr = a.tiles[t];
-            tile = tr.tile;
-            return a.grids[tr.grid];
-        }
-        tile = t;
-        return a.grid;
-    };
-
     // every thread waits on the mbarrier itself (the completed phase makes the
-    // TMA bytes visible to it); the barrier after the wait only agrees on s_err
+    // TMA bytes visible to it); the barrier after the wait also agrees on s_err
     uint32_t phase = 0;
     auto wait_box = [&](bool tma) {
         if (tma) {
@@ -210,27 +118,49 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
         }
         __syncthreads();
     };
-    int t = blockIdx.x;
-    {
-        bool tma = false;
-        if (t < ntiles) {
-            int tile;
-            GridDev g0 = grid_of(t, tile);
-            issue_tile_load<PREC, G, SW, SH, NT>(g0, a.stage, cur, tile, IN, &s_bar, tid);
-            tma = g0.tmap != nullptr;
+    // single grid: start the halo-box load of tile t (every thread: the
+    // plain path loads cooperatively)
+    auto start_single = [&](int t) -> bool {
+        if (tid == 0 && a.grid.tmap) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue_tile_load<PREC, G, SW, SH, NT>(a.grid, a.stage, cur, t, IN, &s_bar, tid);
+        return a.grid.tmap != nullptr;
+    };
+    const int stride = gridDim.x;
+    int t = blockIdx.x, slot = 0;
+    if (t < ntiles && batched) {
+        if (tid < 32) {
+            const TileRef r0 = a.tiles[t];
+            start_batched_tile<PREC, G, SW, SH, NT>(a, &s_hdr[0], r0, hdr_word(a, r0, tid), cur, IN, &s_bar, tid);
+            if (tid == 0 && t + stride < ntiles) s_ref_next = a.tiles[t + stride];
         }
-        wait_box(tma);
+        wait_box(true);
+    } else {
+        wait_box(t < ntiles ? start_single(t) : false);
     }
-    // single grid: the stage-3 wave-speed max is reduced once per CTA
+    // single grid: the stage-3 wave-speed max is reduced once per CTA, and the
+    // step control, the same for every tile, is read once (the leader is CTA
+    // 0, whose first tile is tile 0)
     double lacc = 0.0;
-    for (; t < ntiles; t += gridDim.x) {
-        int tile;
-        const GridDev gd = grid_of(t, tile);
+    TileCtl ctl1{};
+    if (!batched && t < ntiles) ctl1 = tile_control<PREC>(a.grid.ctrl, a.stage, tid == 0 && t == 0);
+    for (; t < ntiles; t += stride, slot ^= 1) {
+        // warp 0 of a batched launch: the next tile's descriptor word and the
+        // entry of the tile after it, in flight during the conversion
+        const bool has_next = t + stride < ntiles;
+        unsigned long long wnext = 0ull;
+        TileRef ref_next{}, ref_after{};
+        if (batched && tid < 32) {
+            if (has_next) {
+                ref_next = s_ref_next;
+                wnext = hdr_word(a, ref_next, tid);
+            }
+            if (t + 2 * stride < ntiles) ref_after = a.tiles[t + 2 * stride];
+        }
+        const GridDev &gd = tile_grid<BATCHED>(s_hdr[slot], a);
+        const int tile = batched ? s_hdr[slot].tile : t;
+        const TileCtl ctl = batched ? s_hdr[slot].ctl : ctl1;
         const int n = gd.n;
         const int tx0 = (tile % gd.tiles_x) * TX, ty0 = (tile / gd.tiles_x) * TY;
-        // ---- 1. the tile's halo box has landed in IN; convert into W --------
-        // (the step control is read by every thread: only the leader writes)
-        const TileCtl ctl = tile_control<PREC>(gd.ctrl, a.stage, tid == 0 && tile == 0);
         const Gas<R> gs{R(gd.gam), R(gd.gam) - R(1)};
         const GasF<R> gf{R(gd.gam), R(1.0 / (gd.gam - 1.0)), R(gd.gam) - R(1)};
         if (s_err) {
@@ -247,21 +177,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
                 const int r = k / SW, c = k - r * SW;
                 const bool ce = ((unsigned)(r - G) < (unsigned)TY && (unsigned)(c - (G - 1)) < (unsigned)(TX + 2)) ||
                                 ((r == G - 1 || r == G + TY) && (unsigned)(c - G) < (unsigned)TX);
-                if constexpr (PREC == P32C) {
-                    if (a.stage >= 2) {
-                        w0 += IN[4 * PL + k]; w1 += IN[5 * PL + k]; w2 += IN[6 * PL + k]; w3 += IN[7 * PL + k];
-                    }
-                    const float ir = frcp(w0);
-                    const float E = w3;
-                    w1 *= ir;
-                    w2 *= ir;
-                    w3 = gf.gm1 * (E - 0.5f * w0 * (w1 * w1 + w2 * w2));
-                    if (ce) {
-                        const float cs2 = gf.gam * w3 * ir;
-                        W[4 * PL + k] = fsqrt(cs2 > 1e-14f ? cs2 : 1e-14f);
-                        W[5 * PL + k] = E;
-                    }
-                } else if constexpr (FAST) {
+                if constexpr (FAST) {
                     if (ce) {
                         R cc, ee;
                         cell_ce<R>(w0, w1, w2, w3, gf, cc, ee);
@@ -274,33 +190,23 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
         }
         __syncthreads();
         // ---- 2. load the next tile into IN (asynchronous through TMA) -------
+        // (the fence orders this CTA's reads of IN before the async-proxy
+        // writes; in a batched launch warp 0 also fetches that tile's header)
         bool next_tma = false;
-        {
-            const int tn = t + gridDim.x;
-            if (tn < ntiles) {
-                int tilen;
-                const GridDev gn = grid_of(tn, tilen);
-                // order this CTA's reads of IN before the async-proxy writes
-                if (tid == 0 && gn.tmap) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                issue_tile_load<PREC, G, SW, SH, NT>(gn, a.stage, cur, tilen, IN, &s_bar, tid);
-                next_tma = gn.tmap != nullptr;
+        if (has_next) {
+            if (batched) {
+                if (tid < 32) {
+                    start_batched_tile<PREC, G, SW, SH, NT>(a, &s_hdr[slot ^ 1], ref_next, wnext, cur, IN, &s_bar,
+                                                            tid);
+                    if (tid == 0) s_ref_next = ref_after;
+                }
+                next_tma = true;
+            } else {
+                next_tma = start_single(t + stride);
             }
         }
 
         if (!ctl.run) {
-            if constexpr (PREC == P32C) if (ctl.copy) {
-                // skipped F32C step: the next step reads the other buffer
-                const float *hi = (const float *)gd.st[cur], *lo = (const float *)gd.lo[cur];
-                for (int k = tid; k < TX * TY; k += NT) {
-                    int r = k / TX, c = k - r * TX, i = tx0 + c, j = ty0 + r;
-                    if (i >= n || j >= n) continue;
-                    float vh[4], vl[4];
-                    long long e = gidx(gd, 0, j, i);
-                    for (int q = 0; q < 4; ++q) { vh[q] = hi[e + q * gd.plane]; vl[q] = lo[e + q * gd.plane]; }
-                    put_cell<float>(gd, (float *)gd.st[nxt], j, i, vh);
-                    put_cell<float>(gd, (float *)gd.lo[nxt], j, i, vl);
-                }
-            }
             wait_box(next_tma);
             continue;
         }
@@ -340,46 +246,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
                 ((R *)a.lam)[kk] = dabs<R>(W[PL + sc]) + dabs<R>(W[2 * PL + sc]) + sound<R>(W[3 * PL + sc], W[sc], gs);
                 continue;
             }
-            if constexpr (PREC == P32C) {
-                const long long e = gidx(gd, 0, j, i);
-                if (a.stage == 1) {
-                    float d[4];
-                    for (int q = 0; q < 4; ++q) d[q] = dt * res[q];
-                    put_cell<float>(gd, (float *)gd.k1, j, i, d);
-                } else if (a.stage == 2) {
-                    const float *d1 = (const float *)gd.k1;
-                    float d[4];
-                    for (int q = 0; q < 4; ++q) d[q] = 0.25f * (d1[e + q * gd.plane] + dt * res[q]);
-                    put_cell<float>(gd, (float *)gd.k2, j, i, d);
-                } else {
-                    const float *d2 = (const float *)gd.k2;
-                    const float *hi = (const float *)gd.st[cur], *lo = (const float *)gd.lo[cur];
-                    float vh[4], vl[4];
-                    for (int q = 0; q < 4; ++q) {
-                        float d = (2.0f / 3.0f) * (d2[e + q * gd.plane] + dt * res[q]);
-                        vh[q] = hi[e + q * gd.plane];
-                        vl[q] = lo[e + q * gd.plane];
-                        df_add(vh[q], vl[q], d);
-                    }
-                    // floors rho, p >= 1e-14 on the new state
-                    float w[4];
-                    {
-                        const float ir = frcp(vh[0]);
-                        w[0] = vh[0]; w[1] = vh[1] * ir; w[2] = vh[2] * ir;
-                        w[3] = gf.gm1 * (vh[3] - 0.5f * (vh[1] * vh[1] + vh[2] * vh[2]) * ir);
-                    }
-                    if (!(w[0] > 1e-14f)) { vh[0] = 1e-14f; vl[0] = 0.f; w[0] = 1e-14f; }
-                    if (!(w[3] > 1e-14f)) {
-                        float ke = 0.5f * (vh[1] * vh[1] + vh[2] * vh[2]) / vh[0];
-                        vh[3] = 1e-14f / gs.gm1 + ke; vl[3] = 0.f; w[3] = 1e-14f;
-                    }
-                    put_cell<float>(gd, (float *)gd.st[nxt], j, i, vh);
-                    put_cell<float>(gd, (float *)gd.lo[nxt], j, i, vl);
-                    float cs2 = gf.gam * w[3] * frcp(w[0]);
-                    float lam = fabsf(w[1]) + fabsf(w[2]) + fsqrt(cs2 > 1e-14f ? cs2 : 1e-14f);
-                    lmax = fmax(lmax, (double)lam);
-                }
-            } else {
+            {
                 // primitive-state modes (F64 / F32): the reference's update
                 R wk[4], w0[4], c0[4], cv[4], w[4];
 #pragma unroll
@@ -450,16 +317,12 @@ __global__ void __launch_bounds__(NT, MinBlocks<PREC>::v) stage_kernel(const __g
         if (a.stage == 3) {
             if (tid == 0 && tile == 0) leader_finish<PREC>(gd.ctrl);
             if (batched) {
-                // tiles of one CTA belong to different instances: per tile
+                // tiles of one CTA belong to different grids: one atomic per
+                // warp and tile
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-                if ((tid & 31) == 0) s_red[tid >> 5] = lmax;
-                __syncthreads();
-                if (tid == 0) {
-                    double m = 0.0;
-                    for (int w = 0; w < NW; ++w) m = fmax(m, s_red[w]);
-                    atomicMax(&gd.ctrl->lam_acc, (unsigned long long)__double_as_longlong(m));
-                }
+                if ((tid & 31) == 0 && lmax > 0.0)
+                    atomicMax(&gd.ctrl->lam_acc, (unsigned long long)__double_as_longlong(lmax));
             } else {
                 lacc = fmax(lacc, lmax);
             }
@@ -493,15 +356,16 @@ struct K {
     using R = typename PrecT<PREC>::R;
     static size_t smem()
     {
-        const int nin = PREC == P32C ? 8 : 4;
-        return sizeof(R) * ((nin + 6) * (ts.ty + 2 * G) * (ts.tx + 2 * G) + 4 * ts.ty * (ts.tx + 1) +
+        return sizeof(R) * (10 * (ts.ty + 2 * G) * (ts.tx + 2 * G) + 4 * ts.ty * (ts.tx + 1) +
                             4 * (ts.ty + 1) * ts.tx);
     }
-    static void *fn() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt>; }
+    static void *fn() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt, false>; }
+    static void *fn_batched() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt, true>; }
 };
 
 struct KernelEntry {
-    void *fn;
+    void *fn;          // single grid
+    void *fn_batched;  // tile table
     size_t smem;
     int nt;
     int ready;
@@ -511,8 +375,14 @@ struct KernelEntry {
 template <int PREC, int ORDER, int SHAPE>
 static KernelEntry entry()
 {
-    return KernelEntry{K<PREC, ORDER, SHAPE>::fn(), K<PREC, ORDER, SHAPE>::smem(),
-                       kTileShapes[SHAPE].nt, 0, 0};
+    return KernelEntry{K<PREC, ORDER, SHAPE>::fn(), K<PREC, ORDER, SHAPE>::fn_batched(),
+                       K<PREC, ORDER, SHAPE>::smem(), kTileShapes[SHAPE].nt, 0, 0};
+}
+
+static KernelEntry entry32c(int shape)
+{
+    return KernelEntry{stage32c_fn(shape, false), stage32c_fn(shape, true), stage32c_smem(shape),
+                       kTileShapes[shape].nt, 0, 0};
 }
 
 #define FVB_SHAPES(P, O) entry<P, O, 0>(), entry<P, O, 1>(), entry<P, O, 2>(), entry<P, O, 3>()
@@ -523,7 +393,7 @@ static KernelEntry *table_for(int prec, int order)
     static KernelEntry t64_5[] = {FVB_SHAPES(P64, 5)};
     static KernelEntry t64_3[] = {FVB_SHAPES(P64, 3)};
     static KernelEntry t32_7[] = {FVB_SHAPES(P32, 7)};
-    static KernelEntry t32c_7[] = {FVB_SHAPES(P32C, 7)};
+    static KernelEntry t32c_7[] = {entry32c(0), entry32c(1), entry32c(2), entry32c(3)};
     if (prec == P64) return order == 7 ? t64_7 : order == 5 ? t64_5 : order == 3 ? t64_3 : nullptr;
     if (order != 7) return nullptr;
     return prec == P32 ? t32_7 : prec == P32C ? t32c_7 : nullptr;
@@ -532,11 +402,15 @@ static KernelEntry *table_for(int prec, int order)
 static cudaError_t prepare(KernelEntry &e)
 {
     if (e.ready) return cudaSuccess;
-    cudaError_t err = cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem);
-    if (err != cudaSuccess) return err;
-    int nb = 0;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, e.fn, e.nt, e.smem);
-    if (err != cudaSuccess) return err;
+    int nb = 1 << 30;
+    for (void *f : {e.fn, e.fn_batched}) {
+        cudaError_t err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem);
+        if (err != cudaSuccess) return err;
+        int k = 0;
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, f, e.nt, e.smem);
+        if (err != cudaSuccess) return err;
+        nb = std::min(nb, k);
+    }
     e.max_ctas = nb;
     e.ready = 1;
     return cudaSuccess;
@@ -616,7 +490,7 @@ cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int
     if (err != cudaSuccess) return err;
     if (grid_ctas <= 0) return cudaSuccess;
     void *args[] = {(void *)&a};
-    return cudaLaunchKernel(e.fn, dim3(grid_ctas), dim3(e.nt), args, e.smem, s);
+    return cudaLaunchKernel(a.grids ? e.fn_batched : e.fn, dim3(grid_ctas), dim3(e.nt), args, e.smem, s);
 }
 
 }  // namespace fvb

@@ -1,0 +1,340 @@
+// fvb_stage32c.cu -- the SSP-RK3 stage kernel of the FP32-compensated form.
+//
+// Same tile pipeline as the FP64 kernel (fvb_stage.cu): persistent CTAs walk
+// the tiles of one grid or of a batch's tile table; the halo box of the next
+// tile streams in through TMA while the current one is computed; every face
+// is evaluated once; the RK combination stores the interior and its ghost
+// images; stage 3 max-reduces the wave speed into the step control.
+//
+// What differs, for FP32 throughput: the faces are evaluated in pairs --
+// x-face p in the low half and y-face p in the high half of packed FP32
+// registers (fvb_face2.cuh) -- so the face arithmetic issues one instruction
+// per two faces; and three CTAs of 256 threads share an SM (68 KB of shared
+// memory and <= 85 registers each).
+//
+// State: conserved (rho, rho u, rho v, E) as an FP32 hi/lo pair per value;
+// the stages form increments d1 = dt L(U0), d2 = (d1 + dt L(U1)) / 4 and add
+// U = U0 + 2/3 (d2 + dt L(U2)) to the pair with an error-free sum, so the
+// state keeps ~48 bits while all flux arithmetic is FP32.  Ping-pong state
+// buffers (parity) keep U0 readable while U is written.
+#include <stdint.h>
+
+#include "fvb_internal.h"
+#include "fvb_physics.cuh"
+#include "fvb_device.cuh"
+#include "fvb_tma.cuh"
+#include "fvb_face2.cuh"
+
+namespace fvb {
+
+// resident CTAs per SM the kernel is compiled for: 768 threads (24 warps)
+// per SM, <= 85 registers a thread
+template <int NT> struct MinBlocks32c { static constexpr int v = 768 / NT; };
+
+template <int TX, int TY, int NT, bool BATCHED>
+__global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const __grid_constant__ StageArgs a)
+{
+    constexpr int G = 4;
+    constexpr int SW = TX + 2 * G, SH = TY + 2 * G, PL = SW * SH;
+    constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1);
+    constexpr int NP = NXF > NYF ? NXF : NYF;
+    constexpr int NC = TX * TY;
+    constexpr int NW = NT / 32;
+
+    // IN: the halo box as loaded (hi + increment planes); W: rho, u, v, p,
+    // c, E the faces read; FX / FY: face fluxes
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float *IN = reinterpret_cast<float *>(smem_raw);
+    float *W = IN + 8 * PL;
+    float *FX = W + 6 * PL;               // [4][TY][TX+1]
+    float *FY = FX + 4 * TY * (TX + 1);   // [4][TY+1][TX]
+    __shared__ double s_red[NW];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ int s_err;
+    __shared__ __align__(16) TileHdr s_hdr[2];
+    __shared__ TileRef s_ref_next;  // batched: table entry of the CTA's next tile
+
+    const int tid = threadIdx.x;
+    constexpr bool batched = BATCHED;
+    const int ntiles = batched ? *a.ntiles : a.ntiles_static;
+    const int cur = a.parity, nxt = a.parity ^ 1;
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        s_err = 0;
+    }
+    __syncthreads();
+
+    // every thread waits on the mbarrier itself (the completed phase makes the
+    // TMA bytes visible to it); the barrier after the wait also agrees on s_err
+    uint32_t phase = 0;
+    auto wait_box = [&](bool tma) {
+        if (tma) {
+            if (mbar_wait(&s_bar, phase)) phase ^= 1;
+            else s_err = 1;
+        }
+        __syncthreads();
+    };
+    // single grid: start the halo-box load of tile t (every thread: the
+    // plain path loads cooperatively)
+    auto start_single = [&](int t) -> bool {
+        if (tid == 0 && a.grid.tmap) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue_tile_load<P32C, G, SW, SH, NT>(a.grid, a.stage, cur, t, IN, &s_bar, tid);
+        return a.grid.tmap != nullptr;
+    };
+    const int stride = gridDim.x;
+    int t = blockIdx.x, slot = 0;
+    if (t < ntiles && batched) {
+        if (tid < 32) {
+            const TileRef r0 = a.tiles[t];
+            start_batched_tile<P32C, G, SW, SH, NT>(a, &s_hdr[0], r0, hdr_word(a, r0, tid), cur, IN, &s_bar, tid);
+            if (tid == 0 && t + stride < ntiles) s_ref_next = a.tiles[t + stride];
+        }
+        wait_box(true);
+    } else {
+        wait_box(t < ntiles ? start_single(t) : false);
+    }
+    double lacc = 0.0;
+    // one grid: the step control is the same for every tile of the launch,
+    // read once (the leader is CTA 0, whose first tile is tile 0)
+    TileCtl ctl1{};
+    if (!batched && t < ntiles) ctl1 = tile_control<P32C>(a.grid.ctrl, a.stage, tid == 0 && t == 0);
+    for (; t < ntiles; t += stride, slot ^= 1) {
+        // warp 0 of a batched launch: the next tile's descriptor word and the
+        // entry of the tile after it, in flight during the conversion
+        const bool has_next = t + stride < ntiles;
+        unsigned long long wnext = 0ull;
+        TileRef ref_next{}, ref_after{};
+        if (batched && tid < 32) {
+            if (has_next) {
+                ref_next = s_ref_next;
+                wnext = hdr_word(a, ref_next, tid);
+            }
+            if (t + 2 * stride < ntiles) ref_after = a.tiles[t + 2 * stride];
+        }
+        const GridDev &gd = tile_grid<BATCHED>(s_hdr[slot], a);
+        const int tile = batched ? s_hdr[slot].tile : t;
+        const TileCtl ctl = batched ? s_hdr[slot].ctl : ctl1;
+        const int n = gd.n;
+        const int tx0 = (tile % gd.tiles_x) * TX, ty0 = (tile / gd.tiles_x) * TY;
+        const float gam = (float)gd.gam, gm1 = (float)gd.gam - 1.0f, igm1 = (float)(1.0 / (gd.gam - 1.0));
+        if (s_err) {
+            if (tid == 0 && gd.ctrl) gd.ctrl->status = FVB_ERR_TIMEOUT;
+            break;
+        }
+        // ---- 1. stage input U0 + d into W as primitives (+ c, E where the
+        //         HLLE reads them: interior rows x columns [G-1, G+TX], and
+        //         rows G-1, G+TY x the interior columns) --------------------
+        if (ctl.run) {
+            for (int k = tid; k < PL; k += NT) {
+                float w0 = IN[k], w1 = IN[PL + k], w2 = IN[2 * PL + k], w3 = IN[3 * PL + k];
+                if (a.stage >= 2) {
+                    w0 += IN[4 * PL + k]; w1 += IN[5 * PL + k]; w2 += IN[6 * PL + k]; w3 += IN[7 * PL + k];
+                }
+                const int r = k / SW, c = k - r * SW;
+                const bool ce = ((unsigned)(r - G) < (unsigned)TY && (unsigned)(c - (G - 1)) < (unsigned)(TX + 2)) ||
+                                ((r == G - 1 || r == G + TY) && (unsigned)(c - G) < (unsigned)TX);
+                const float ir = frcp(w0);
+                const float E = w3;
+                w1 *= ir;
+                w2 *= ir;
+                w3 = gm1 * (E - 0.5f * w0 * (w1 * w1 + w2 * w2));
+                if (ce) {
+                    const float cs2 = gam * w3 * ir;
+                    W[4 * PL + k] = fsqrt(cs2 > 1e-14f ? cs2 : 1e-14f);
+                    W[5 * PL + k] = E;
+                }
+                W[k] = w0; W[PL + k] = w1; W[2 * PL + k] = w2; W[3 * PL + k] = w3;
+            }
+        }
+        __syncthreads();
+        // ---- 2. load the next tile into IN (asynchronous through TMA) -------
+        // (in a batched launch warp 0 also fetches that tile's header)
+        bool next_tma = false;
+        if (has_next) {
+            if (batched) {
+                if (tid < 32) {
+                    start_batched_tile<P32C, G, SW, SH, NT>(a, &s_hdr[slot ^ 1], ref_next, wnext, cur, IN, &s_bar,
+                                                            tid);
+                    if (tid == 0) s_ref_next = ref_after;
+                }
+                next_tma = true;
+            } else {
+                next_tma = start_single(t + stride);
+            }
+        }
+        if (!ctl.run) {
+            if (ctl.copy) {
+                // skipped step: the next step reads the other buffer
+                const float *hi = (const float *)gd.st[cur], *lo = (const float *)gd.lo[cur];
+                for (int k = tid; k < NC; k += NT) {
+                    int r = k / TX, c = k - r * TX, i = tx0 + c, j = ty0 + r;
+                    if (i >= n || j >= n) continue;
+                    float vh[4], vl[4];
+                    long long e = gidx(gd, 0, j, i);
+                    for (int q = 0; q < 4; ++q) { vh[q] = hi[e + q * gd.plane]; vl[q] = lo[e + q * gd.plane]; }
+                    put_cell<float>(gd, (float *)gd.st[nxt], j, i, vh);
+                    put_cell<float>(gd, (float *)gd.lo[nxt], j, i, vl);
+                }
+            }
+            wait_box(next_tma);
+            continue;
+        }
+        const float dt = (float)ctl.dt;
+        const float inv_h = (float)(1.0 / gd.h);
+
+        // ---- 3. face fluxes, x-face p and y-face p as one packed pair -------
+        for (int p = tid; p < NP; p += NT) {
+            const int px = p < NXF ? p : NXF - 1, py = p < NYF ? p : NYF - 1;
+            const int rx = px / (TX + 1), cx = px - rx * (TX + 1);
+            const int ry = py / TX, cy = py - ry * TX;
+            const int bx = (rx + G) * SW + (cx + G), by = (ry + G) * SW + (cy + G);
+            f2::V L[4], Rv[4], WL[4], WR[4];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                // x lane: (rho, u, v, p) along x; y lane: (rho, v, u, p) along y
+                const float *vx = W + m * PL + bx;
+                const float *vy = W + (m == 1 ? 2 : m == 2 ? 1 : m) * PL + by;
+                f2::V s[8];
+#pragma unroll
+                for (int d = 0; d < 8; ++d) s[d] = make_float2(vx[d - G], vy[(d - G) * SW]);
+                f2::upface7(s, L[m], Rv[m]);
+                WL[m] = s[G - 1];
+                WR[m] = s[G];
+            }
+            const f2::V tiny = f2::splat(1e-14f);
+            L[0] = f2::vmax(L[0], tiny); Rv[0] = f2::vmax(Rv[0], tiny);
+            L[3] = f2::vmax(L[3], tiny); Rv[3] = f2::vmax(Rv[3], tiny);
+            const float *cex = W + 4 * PL + bx, *cey = W + 4 * PL + by;
+            f2::V F[4];
+            f2::face_flux(L, Rv, WL, WR, make_float2(cex[-1], cey[-SW]), make_float2(cex[0], cey[0]),
+                          make_float2(cex[PL - 1], cey[PL - SW]), make_float2(cex[PL], cey[PL]), gam, igm1, F);
+            if (p < NXF) {
+                float *o = FX + rx * (TX + 1) + cx;
+                constexpr int os = TY * (TX + 1);
+                o[0] = F[0].x; o[os] = F[1].x; o[2 * os] = F[2].x; o[3 * os] = F[3].x;
+            }
+            if (p < NYF) {
+                float *o = FY + ry * TX + cy;
+                constexpr int os = (TY + 1) * TX;
+                // y lane: normal momentum is v, tangential u
+                o[0] = F[0].y; o[os] = F[2].y; o[2 * os] = F[1].y; o[3 * os] = F[3].y;
+            }
+        }
+        __syncthreads();
+
+        // ---- 4. divergence, RK combination, stores --------------------------
+        double lmax = 0.0;
+        for (int k = tid; k < NC; k += NT) {
+            const int r = k / TX, c = k - r * TX, i = tx0 + c, j = ty0 + r;
+            if (i >= n || j >= n) continue;
+            float res[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float *fx = FX + q * TY * (TX + 1) + r * (TX + 1) + c;
+                const float *fy = FY + q * (TY + 1) * TX + r * TX + c;
+                res[q] = -(fx[1] - fx[0]) * inv_h - (fy[TX] - fy[0]) * inv_h;
+            }
+            if (a.stage == 1) {
+                float d[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) d[q] = dt * res[q];
+                put_cell<float>(gd, (float *)gd.k1, j, i, d);
+            } else if (a.stage == 2) {
+                float d[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float d1 = ((const float *)gd.k1)[gidx(gd, q, j, i)];
+                    d[q] = 0.25f * (d1 + dt * res[q]);
+                }
+                put_cell<float>(gd, (float *)gd.k2, j, i, d);
+            } else {
+                float vh[4], vl[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const long long e = gidx(gd, q, j, i);
+                    const float d = (2.0f / 3.0f) * (((const float *)gd.k2)[e] + dt * res[q]);
+                    vh[q] = ((const float *)gd.st[cur])[e];
+                    vl[q] = ((const float *)gd.lo[cur])[e];
+                    df_add(vh[q], vl[q], d);
+                }
+                // floors rho, p >= 1e-14 on the new state
+                float w[4];
+                {
+                    const float ir = frcp(vh[0]);
+                    w[0] = vh[0]; w[1] = vh[1] * ir; w[2] = vh[2] * ir;
+                    w[3] = gm1 * (vh[3] - 0.5f * (vh[1] * vh[1] + vh[2] * vh[2]) * ir);
+                }
+                if (!(w[0] > 1e-14f)) { vh[0] = 1e-14f; vl[0] = 0.f; w[0] = 1e-14f; }
+                if (!(w[3] > 1e-14f)) {
+                    float ke = 0.5f * (vh[1] * vh[1] + vh[2] * vh[2]) / vh[0];
+                    vh[3] = 1e-14f / gm1 + ke; vl[3] = 0.f; w[3] = 1e-14f;
+                }
+                put_cell<float>(gd, (float *)gd.st[nxt], j, i, vh);
+                put_cell<float>(gd, (float *)gd.lo[nxt], j, i, vl);
+                float cs2 = gam * w[3] * frcp(w[0]);
+                float lam = fabsf(w[1]) + fabsf(w[2]) + fsqrt(cs2 > 1e-14f ? cs2 : 1e-14f);
+                lmax = fmax(lmax, (double)lam);
+            }
+        }
+
+        // ---- 5. max wave speed of the new state (stage 3) ------------------
+        if (a.stage == 3) {
+            if (tid == 0 && tile == 0) leader_finish<P32C>(gd.ctrl);
+            if (batched) {
+                // tiles of one CTA belong to different grids: one atomic per
+                // warp and tile
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+                if ((tid & 31) == 0 && lmax > 0.0)
+                    atomicMax(&gd.ctrl->lam_acc, (unsigned long long)__double_as_longlong(lmax));
+            } else {
+                lacc = fmax(lacc, lmax);
+            }
+        }
+        // ---- 6. next tile's halo box: wait, then release W / FX / FY --------
+        wait_box(next_tma);
+    }
+    if (!batched && a.stage == 3) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lacc = fmax(lacc, __shfl_xor_sync(0xffffffffu, lacc, o));
+        if ((tid & 31) == 0) s_red[tid >> 5] = lacc;
+        __syncthreads();
+        if (tid == 0 && a.grid.ctrl) {
+            double m = 0.0;
+            for (int w = 0; w < NW; ++w) m = fmax(m, s_red[w]);
+            if (m > 0.0) atomicMax(&a.grid.ctrl->lam_acc, (unsigned long long)__double_as_longlong(m));
+        }
+    }
+    // a load still in flight after an error: wait for it (bounded) so no
+    // copy into this CTA's shared memory outlives it
+    if (s_err && gd_has_tma(a)) mbar_wait(&s_bar, phase);
+}
+
+template <int SHAPE>
+static void *fn32c(bool batched)
+{
+    constexpr TileShape ts = kTileShapes[SHAPE];
+    return batched ? (void *)stage32c_kernel<ts.tx, ts.ty, ts.nt, true>
+                   : (void *)stage32c_kernel<ts.tx, ts.ty, ts.nt, false>;
+}
+
+void *stage32c_fn(int shape, bool batched)
+{
+    switch (shape) {
+    case 0: return fn32c<0>(batched);
+    case 1: return fn32c<1>(batched);
+    case 2: return fn32c<2>(batched);
+    case 3: return fn32c<3>(batched);
+    default: return nullptr;
+    }
+}
+
+size_t stage32c_smem(int shape)
+{
+    if (shape < 0 || shape >= kNumTileShapes) return 0;
+    const TileShape &ts = kTileShapes[shape];
+    const int sw = ts.tx + 8, sh = ts.ty + 8;
+    return sizeof(float) * ((size_t)14 * sw * sh + 4 * ts.ty * (ts.tx + 1) + 4 * (ts.ty + 1) * ts.tx);
+}
+
+}  // namespace fvb
