@@ -41,6 +41,7 @@ struct fvb_batch {
     std::vector<Instance> inst;
     Ctrl *ctrl_dev = nullptr;       // [max_inst]
     Ctrl *ctrl_host = nullptr;      // pinned mirror
+    TileCtl *ctls_dev = nullptr;    // [max_inst] step control of the stage being launched
     GridDev *desc_dev = nullptr;    // [max_inst]
     GridDev *desc_host = nullptr;   // pinned staging
     TileRef *tiles_dev = nullptr;
@@ -69,6 +70,7 @@ static StageArgs batch_args(const fvb_batch *b, int stage, int parity)
 {
     StageArgs a{};
     a.grids = b->desc_dev;
+    a.ctls = b->ctls_dev;
     a.tiles = b->tiles_dev;
     a.ntiles = b->ntiles_dev;
     a.stage = stage;
@@ -80,7 +82,10 @@ static cudaError_t launch_steps(fvb_batch *b, int nsteps)
 {
     for (int k = 0; k < nsteps; ++k) {
         for (int stage = 1; stage <= 3; ++stage) {
-            cudaError_t e = launch_stage(b->prec, b->order, b->shape, batch_args(b, stage, b->parity), b->ctas,
+            // every slot's step control for this stage, then the stage
+            cudaError_t e = launch_stage_control(b->prec, b->ctrl_dev, b->max_inst, stage, b->ctls_dev, b->stream);
+            if (e != cudaSuccess) return e;
+            e = launch_stage(b->prec, b->order, b->shape, batch_args(b, stage, b->parity), b->ctas,
                                          b->stream);
             if (e != cudaSuccess) return e;
         }
@@ -194,6 +199,7 @@ fvb_status fvb_batch_create(const fvb_batch_config *cfg, fvb_batch **out)
     e = cudaMalloc(&b->ctrl_dev, sizeof(Ctrl) * b->max_inst);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->ctrl_dev, 0, sizeof(Ctrl) * b->max_inst, b->stream);
     if (e == cudaSuccess) e = cudaMallocHost(&b->ctrl_host, sizeof(Ctrl) * b->max_inst);
+    if (e == cudaSuccess) e = cudaMalloc(&b->ctls_dev, sizeof(TileCtl) * b->max_inst);
     if (e == cudaSuccess) e = cudaMalloc(&b->desc_dev, sizeof(GridDev) * b->max_inst);
     if (e == cudaSuccess) e = cudaMallocHost(&b->desc_host, sizeof(GridDev) * b->max_inst);
     if (e == cudaSuccess) e = cudaMalloc(&b->ntiles_dev, sizeof(int));
@@ -219,6 +225,7 @@ void fvb_batch_destroy(fvb_batch *b)
         if (I.block) cudaFree(I.block);
     cudaFree(b->ctrl_dev);
     cudaFreeHost(b->ctrl_host);
+    cudaFree(b->ctls_dev);
     cudaFree(b->desc_dev);
     cudaFreeHost(b->desc_host);
     cudaFree(b->tiles_dev);
@@ -437,9 +444,11 @@ fvb_status fvb_batch_remove(fvb_batch *b, int id)
         if (st) return st;
     }
     cudaFreeAsync(I.block, b->stream);
+    // a zero step control is inactive: the stage-control kernel leaves it be
+    cudaError_t e = cudaMemsetAsync(b->ctrl_dev + id, 0, sizeof(Ctrl), b->stream);
     b->in_use -= I.bytes;
     I = Instance();
-    return FVB_OK;
+    return e == cudaSuccess ? FVB_OK : cuda_fail(e, "step control reset");
 }
 
 }  // extern "C"

@@ -83,12 +83,6 @@ __device__ __forceinline__ bool gd_has_tma(const StageArgs &a)
     return a.grids != nullptr || a.grid.tmap != nullptr;
 }
 
-struct TileCtl {
-    double dt;
-    int run;    // compute the stage on this tile
-    int copy;   // F32C stage 3 of a skipped step: carry the state across
-};
-
 // Step control, evaluated by thread 0 of each CTA for its tile's grid.
 template <int PREC>
 __device__ TileCtl tile_control(Ctrl *c, int stage, bool leader)

@@ -63,9 +63,19 @@ struct TileRef {
 
 enum Prec { P64 = 0, P32 = 1, P32C = 2 };
 
+// Step control of one grid for one RK stage: the dt the stage uses, whether
+// its tiles compute, and (FP32c stage 3 of a grid that stopped) whether they
+// carry the state to the other buffer.
+struct TileCtl {
+    double dt;
+    int run;
+    int copy;
+};
+
 struct StageArgs {
     GridDev grid;              // single-grid launches
     const GridDev *grids;      // batched launches: grid descriptors
+    const TileCtl *ctls;       // batched launches: step control of each grid
     const TileRef *tiles;      // batched launches: tile table
     const int *ntiles;         // batched launches: live tile count (device)
     int ntiles_static;         // single-grid launches: tiles
@@ -92,6 +102,12 @@ bool encode_tile_maps(const GridDev &gd, int prec, int order, int shape, CUtenso
 // (fvb_stage32c.cu)
 void *stage32c_fn(int shape, bool batched);
 size_t stage32c_smem(int shape);
+
+// Step control of `count` grids for one stage of a batched launch
+// (fvb_stage.cu): evaluates each grid's Ctrl, applies the stage's control
+// writes (dt in stage 1, the wave-speed accumulator reset in stage 2, the
+// time / step advance in stage 3) and writes the TileCtl the stage reads.
+cudaError_t launch_stage_control(int prec, Ctrl *ctrl, int count, int stage, TileCtl *out, cudaStream_t s);
 
 // launchers (fvb_stage.cu)
 cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int grid_ctas,

@@ -315,7 +315,8 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const __grid_constant__ St
 
         // ---- 5. max wave speed of the new state (stage 3) ------------------
         if (a.stage == 3) {
-            if (tid == 0 && tile == 0) leader_finish<PREC>(gd.ctrl);
+            // (a batched launch advances its grids' time in the stage-control kernel)
+            if (!batched && tid == 0 && tile == 0) leader_finish<PREC>(gd.ctrl);
             if (batched) {
                 // tiles of one CTA belong to different grids: one atomic per
                 // warp and tile
@@ -344,6 +345,31 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const __grid_constant__ St
     // a load still in flight after an error: wait for it (bounded) so no
     // copy into this CTA's shared memory outlives it
     if (s_err && gd_has_tma(a)) mbar_wait(&s_bar, phase);
+}
+
+// ---------------------------------------------------------------------------
+// step control of a batched launch, one thread per grid slot
+// ---------------------------------------------------------------------------
+template <int PREC>
+__global__ void stage_control_kernel(Ctrl *ctrl, int count, int stage, TileCtl *out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    Ctrl *c = ctrl + i;
+    const TileCtl k = tile_control<PREC>(c, stage, true);
+    // the stage-3 tiles read only `active` and `dt`: the time advances here
+    if (stage == 3 && k.run) leader_finish<PREC>(c);
+    out[i] = k;
+}
+
+cudaError_t launch_stage_control(int prec, Ctrl *ctrl, int count, int stage, TileCtl *out, cudaStream_t s)
+{
+    if (count <= 0) return cudaSuccess;
+    const int nt = 128, nb = (count + nt - 1) / nt;
+    if (prec == P64) stage_control_kernel<P64><<<nb, nt, 0, s>>>(ctrl, count, stage, out);
+    else if (prec == P32) stage_control_kernel<P32><<<nb, nt, 0, s>>>(ctrl, count, stage, out);
+    else stage_control_kernel<P32C><<<nb, nt, 0, s>>>(ctrl, count, stage, out);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

@@ -279,7 +279,8 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
 
         // ---- 5. max wave speed of the new state (stage 3) ------------------
         if (a.stage == 3) {
-            if (tid == 0 && tile == 0) leader_finish<P32C>(gd.ctrl);
+            // (a batched launch advances its grids' time in the stage-control kernel)
+            if (!batched && tid == 0 && tile == 0) leader_finish<P32C>(gd.ctrl);
             if (batched) {
                 // tiles of one CTA belong to different grids: one atomic per
                 // warp and tile

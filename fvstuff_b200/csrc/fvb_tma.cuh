@@ -2,6 +2,7 @@
 // the stage kernels (no cluster multicast anywhere), and the tile headers of
 // batched launches.
 #pragma once
+#include <stddef.h>
 #include <stdint.h>
 
 #include "fvb_internal.h"
@@ -100,20 +101,24 @@ __device__ __forceinline__ void issue_tile_load(const GridDev &gd, int stage, in
 // Tile headers of a batched launch.  Warp 0 stages them one tile ahead:
 // the table entry of the CTA's next tile is loaded a tile early, and at the
 // top of each tile each lane of warp 0 loads one 8-byte word of the next
-// tile's grid descriptor, so both loads are in flight while the tile is
-// converted.  After the conversion barrier warp 0 stores the words into
-// shared memory, lane 0 starts the next halo-box load and evaluates that
-// grid's step control; every thread reads the header after the barrier
-// that ends the tile.  (A single-grid launch reads its grid from the kernel
-// parameter and evaluates the step control once: it is the same for every
-// tile.)
+// tile's grid descriptor or of its grid's step control for this stage
+// (written by the stage-control kernel before the launch), so these loads
+// are in flight while the tile is converted.  After the conversion barrier
+// warp 0 stores the words into shared memory and lane 0 starts the next
+// halo-box load; every thread reads the header after the barrier that ends
+// the tile.  (A single-grid launch reads its grid from the kernel parameter
+// and evaluates the step control once: it is the same for every tile.)
 struct TileHdr {
     GridDev gd;
     TileCtl ctl;
     int tile;
     int pad;
 };
-constexpr int kHdrWords = (int)(sizeof(GridDev) / 8);
+constexpr int kGridWords = (int)(sizeof(GridDev) / 8);
+constexpr int kHdrWords = kGridWords + (int)(sizeof(TileCtl) / 8);
+static_assert(sizeof(GridDev) % 8 == 0 && sizeof(TileCtl) % 8 == 0 && kHdrWords <= 32,
+              "one warp copies a header");
+static_assert(offsetof(TileHdr, ctl) == sizeof(GridDev), "grid descriptor and step control are contiguous");
 
 // the grid of the current tile: its header in shared memory (batched) or
 // the kernel parameter (single grid); a reference, so each field is read
@@ -124,11 +129,12 @@ __device__ __forceinline__ const GridDev &tile_grid(const TileHdr &h, const Stag
     if constexpr (BATCHED) return h.gd;
     else return a.grid;
 }
-static_assert(sizeof(GridDev) % 8 == 0 && kHdrWords <= 32, "one warp copies a GridDev");
 
 __device__ __forceinline__ unsigned long long hdr_word(const StageArgs &a, TileRef r, int lane)
 {
-    return lane < kHdrWords ? reinterpret_cast<const unsigned long long *>(a.grids + r.grid)[lane] : 0ull;
+    if (lane < kGridWords) return reinterpret_cast<const unsigned long long *>(a.grids + r.grid)[lane];
+    if (lane < kHdrWords) return reinterpret_cast<const unsigned long long *>(a.ctls + r.grid)[lane - kGridWords];
+    return 0ull;
 }
 
 // warp 0: publish the header of tile r into h and start its halo-box load
@@ -136,22 +142,21 @@ template <int PREC, int G, int SW, int SH, int NT, class R>
 __device__ __forceinline__ void start_batched_tile(const StageArgs &a, TileHdr *h, TileRef r, unsigned long long w,
                                                    int parity, R *IN, uint64_t *bar, int lane)
 {
-    if (lane < kHdrWords) reinterpret_cast<unsigned long long *>(&h->gd)[lane] = w;
+    if (lane < kHdrWords) reinterpret_cast<unsigned long long *>(h)[lane] = w;
     __syncwarp();
     if (lane == 0) {
-        TileCtl c{};
+        h->tile = r.tile;
         if (h->gd.tmap) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             issue_tile_load<PREC, G, SW, SH, NT>(h->gd, a.stage, parity, r.tile, IN, bar, 0);
-            c = tile_control<PREC>(h->gd.ctrl, a.stage, r.tile == 0);
         } else {
             // batched grids load through TMA only: never compute on a box
             // that was not loaded
             mbar_arrive(bar);
+            h->ctl.run = 0;
+            h->ctl.copy = 0;
             if (r.tile == 0) h->gd.ctrl->status = FVB_ERR_INVALID;
         }
-        h->tile = r.tile;
-        h->ctl = c;
     }
     __syncwarp();
 }
