@@ -196,6 +196,16 @@ fvb_status fvb_batch_create(const fvb_batch_config *cfg, fvb_batch **out)
         if (e != cudaSuccess) { delete b; return cuda_fail(e, "stream"); }
         b->own_stream = true;
     }
+    {
+        // instances come and go: keep device memory they free in the
+        // stream-ordered pool for the next one rather than returning it to the
+        // driver at every synchronisation
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, cfg->device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     e = cudaMalloc(&b->ctrl_dev, sizeof(Ctrl) * b->max_inst);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->ctrl_dev, 0, sizeof(Ctrl) * b->max_inst, b->stream);
     if (e == cudaSuccess) e = cudaMallocHost(&b->ctrl_host, sizeof(Ctrl) * b->max_inst);
@@ -206,7 +216,8 @@ fvb_status fvb_batch_create(const fvb_batch_config *cfg, fvb_batch **out)
     if (e == cudaSuccess) e = cudaMallocHost(&b->ntiles_host, sizeof(int));
     if (e != cudaSuccess) { fvb_batch_destroy(b); return cuda_fail(e, "batch allocation"); }
     std::memset(b->desc_host, 0, sizeof(GridDev) * b->max_inst);
-    b->shape = cfg->tile >= 0 ? cfg->tile : autotune_shape(b->prec, 7, 256);
+    // a batched launch walks many tiles, as a large grid does: tune there
+    b->shape = cfg->tile >= 0 ? cfg->tile : autotune_shape(b->prec, 7, 4096);
     int per_sm = stage_max_ctas_per_sm(b->prec, 7, b->shape);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device);
@@ -298,8 +309,7 @@ fvb_status fvb_batch_add(fvb_batch *b, const fvb_instance_desc *d, int *id)
             return fail(FVB_ERR_CUDA, "cannot encode TMA descriptors for n = %d", d->n);
         }
         CUtensorMap *dm = (CUtensorMap *)((char *)I.block + tmap_off);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(dm, maps, sizeof maps, cudaMemcpyHostToDevice, b->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);  // `maps` is a stack copy
+        if (e == cudaSuccess) e = put_tile_maps(maps, dm, b->stream);
         I.gd.tmap = dm;
     }
     // initial state: FP64 primitives on the device, imported into the buffer

@@ -18,49 +18,59 @@ __device__ __forceinline__ long long gidx(const GridDev &gd, int q, int j, int i
     return (long long)q * gd.plane + (long long)(j + gd.g) * gd.pitch + (i + gd.g) + gd.xoff;
 }
 
-// Coordinates of cell i and of every ghost cell that mirrors it along one
-// axis; flip marks reflected images (normal momentum negated).
-__device__ __forceinline__ int mirror_images(int i, int n, int g, int bc, int *pos, bool *flip)
+// Ghost images of cell i along one axis (index 0 is the cell itself).
+//   reflect:      i < g -> -1-i,  i >= n-g -> 2n-1-i  (normal momentum negated)
+//   periodic:     i < g -> i+n,   i >= n-g -> i-n
+//   transmissive: i == 0 -> -1..-g,  i == n-1 -> n..n+g-1
+// (the ghost fills of fv_up7_ducros_2d.cu:338-362 and keep_fv_euler_2d.cu:
+// 224-243, and zero-gradient, seen from the cell side).  Computed
+// arithmetically, so no per-thread arrays are needed.
+__device__ __forceinline__ int n_images(int i, int n, int g, int bc)
 {
-    int k = 0;
-    pos[k] = i; flip[k++] = false;
+    if (bc == FVB_BC_REFLECT || bc == FVB_BC_PERIODIC) return 1 + (i < g) + (i >= n - g);
+    return 1 + (i == 0 ? g : 0) + (i == n - 1 ? g : 0);
+}
+
+__device__ __forceinline__ int image_of(int k, int i, int n, int g, int bc, bool &flip)
+{
+    flip = false;
+    if (k == 0) return i;
+    const bool low = (k == 1 && i < g);
     if (bc == FVB_BC_REFLECT) {
-        if (i < g) { pos[k] = -1 - i; flip[k++] = true; }
-        if (i >= n - g) { pos[k] = 2 * n - 1 - i; flip[k++] = true; }
-    } else if (bc == FVB_BC_PERIODIC) {
-        if (i < g) { pos[k] = i + n; flip[k++] = false; }
-        if (i >= n - g) { pos[k] = i - n; flip[k++] = false; }
-    } else {
-        if (i == 0) for (int m = 1; m <= g; ++m) { pos[k] = -m; flip[k++] = false; }
-        if (i == n - 1) for (int m = 0; m < g; ++m) { pos[k] = n + m; flip[k++] = false; }
+        flip = true;
+        return low ? -1 - i : 2 * n - 1 - i;
     }
-    return k;
+    if (bc == FVB_BC_PERIODIC) return low ? i + n : i - n;
+    if (i == 0 && k <= g) return -k;
+    return n - 1 + (i == 0 ? k - g : k);
 }
 
 // Store a cell value into the interior and all its ghost images.
 template <class R>
 __device__ __forceinline__ void put_cell(const GridDev &gd, R *buf, int j, int i, const R v[4])
 {
-    long long c = gidx(gd, 0, j, i);
+    const long long pl = gd.plane;
+    const long long c = gidx(gd, 0, j, i);
     buf[c] = v[0];
-    buf[c + gd.plane] = v[1];
-    buf[c + 2 * gd.plane] = v[2];
-    buf[c + 3 * gd.plane] = v[3];
+    buf[c + pl] = v[1];
+    buf[c + 2 * pl] = v[2];
+    buf[c + 3 * pl] = v[3];
     const int g = gd.g, n = gd.n;
     if (i >= g && i < n - g && j >= g && j < n - g) return;
-    int xs[12], ys[12];
-    bool fx[12], fy[12];
-    int nx = mirror_images(i, n, g, gd.bcx, xs, fx);
-    int ny = mirror_images(j, n, g, gd.bcy, ys, fy);
-    for (int a = 0; a < ny; ++a)
-        for (int b = 0; b < nx; ++b) {
-            if (a == 0 && b == 0) continue;
-            long long e = gidx(gd, 0, ys[a], xs[b]);
+    const int nx = n_images(i, n, g, gd.bcx), ny = n_images(j, n, g, gd.bcy);
+    for (int ka = 0; ka < ny; ++ka) {
+        bool fy;
+        const int y = image_of(ka, j, n, g, gd.bcy, fy);
+        for (int kb = (ka == 0 ? 1 : 0); kb < nx; ++kb) {
+            bool fx;
+            const int x = image_of(kb, i, n, g, gd.bcx, fx);
+            const long long e = gidx(gd, 0, y, x);
             buf[e] = v[0];
-            buf[e + gd.plane] = fx[b] ? -v[1] : v[1];
-            buf[e + 2 * gd.plane] = fy[a] ? -v[2] : v[2];
-            buf[e + 3 * gd.plane] = v[3];
+            buf[e + pl] = fx ? -v[1] : v[1];
+            buf[e + 2 * pl] = fy ? -v[2] : v[2];
+            buf[e + 3 * pl] = v[3];
         }
+    }
 }
 
 // Error-free sum of a double-float (hi, lo) and a float increment d

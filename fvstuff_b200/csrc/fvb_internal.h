@@ -97,6 +97,8 @@ constexpr TileShape kTileShapes[kNumTileShapes] = {
 // TMA descriptors (fvb_stage.cu): encode the four maps of a grid for a
 // tile shape into host memory; false if this grid cannot use TMA
 bool encode_tile_maps(const GridDev &gd, int prec, int order, int shape, CUtensorMap out[TM_COUNT]);
+// stream-ordered copy of encoded maps into device memory (dst 64-byte aligned)
+cudaError_t put_tile_maps(const CUtensorMap maps[TM_COUNT], CUtensorMap *dst, cudaStream_t s);
 
 // the FP32-compensated stage kernel of a tile shape and its shared memory
 // (fvb_stage32c.cu)

@@ -493,6 +493,28 @@ bool encode_tile_maps(const GridDev &gd, int prec, int order, int shape, CUtenso
     return true;
 }
 
+// Copy a grid's tensor maps into device memory from a kernel parameter, so
+// the host copy need not outlive the call (no stream synchronisation).
+struct TileMaps {
+    CUtensorMap m[TM_COUNT];
+};
+
+__global__ void put_maps_kernel(const __grid_constant__ TileMaps maps, CUtensorMap *dst)
+{
+    constexpr int NV = (int)(sizeof(TileMaps) / 16);
+    const int k = threadIdx.x;
+    if (k < NV) reinterpret_cast<uint4 *>(dst)[k] = reinterpret_cast<const uint4 *>(&maps)[k];
+}
+
+cudaError_t put_tile_maps(const CUtensorMap maps[TM_COUNT], CUtensorMap *dst, cudaStream_t s)
+{
+    static_assert(sizeof(TileMaps) % 16 == 0 && sizeof(TileMaps) / 16 <= 64, "one small block copies the maps");
+    TileMaps tm;
+    for (int m = 0; m < TM_COUNT; ++m) tm.m[m] = maps[m];
+    put_maps_kernel<<<1, 64, 0, s>>>(tm, dst);
+    return cudaGetLastError();
+}
+
 size_t stage_smem_bytes(int prec, int order, int shape)
 {
     KernelEntry *t = table_for(prec, order);
