@@ -39,11 +39,11 @@ METRIC = "cell-stage updates/s on 1 B200 (plain vs batched/served); p50/p99 solv
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=400)
+    p.add_argument("--steps", type=int, default=None, help="timed steps (plain 400, large 2000)")
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="fvb", choices=["fvb", "reference"])
     p.add_argument("--precision", default="f64", choices=["f64", "f32c", "f32"])
-    p.add_argument("--n", type=int, default=2048)
+    p.add_argument("--n", type=int, default=None, help="grid side (plain 2048, large 8192)")
     p.add_argument("--no-forms", action="store_true", help="skip the extra FP32c measurement")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     p.add_argument("--no-e2e", action="store_true")
@@ -55,7 +55,13 @@ def parse():
     p.add_argument("--rate", type=float, default=200.0, help="serve: mean arrivals per second")
     p.add_argument("--max-n", type=int, default=2048, help="serve: largest grid side")
     p.add_argument("--steps-per-round", type=int, default=16, help="serve: batch steps between admissions")
-    return p.parse_args()
+    a = p.parse_args()
+    large = a.mode == "large"
+    if a.n is None:
+        a.n = 8192 if large else 2048
+    if a.steps is None:
+        a.steps = 2000 if large else 400
+    return a
 
 
 def workload(n):

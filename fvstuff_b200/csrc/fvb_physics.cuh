@@ -264,11 +264,8 @@ __device__ __forceinline__ void face_flux_fast(const R L[4], const R Rv[4], cons
                                                R cWR, R EWL, R EWR, const GasF<R> &gs, R F[4])
 {
     const R zero = R(0);
-    // --- HLLC of the reconstructed states ---
-    // branch-free: the one-sided fluxes and the star flux are all formed and
-    // the Davis-bound test selects among them, so the HLLC and HLLE chains
-    // share one basic block and interleave.  In the supersonic cases the
-    // unused star flux may be non-finite; a select never propagates it.
+    // --- HLLC of the reconstructed states (branch-free, so the HLLC and HLLE
+    // chains share one basic block and interleave) ---
     R Fh0, Fh1, Fh2, Fh3;
     {
         const R rL = L[0], uL = L[1], tL = L[2], pL = L[3];
@@ -292,37 +289,37 @@ __device__ __forceinline__ void face_flux_fast(const R L[4], const R Rv[4], cons
         const R SL = dmin<R>(uL - cL, uR - cR), SR = dmax<R>(uL + cL, uR + cR);
         const R dL = rL * (SL - uL), dR = rR * (SR - uR);
         const R Ss = (pR - pL + dL * uL - dR * uR) * frcp(dL - dR);
-        const bool left = (Ss >= zero);
+        // side K: by the contact when subsonic, by the fan when supersonic
+        const bool supL = (SL >= zero);
+        const bool sup = supL || (SR <= zero);
+        const bool left = sup ? supL : (Ss >= zero);
         const R rK = left ? rL : rR, uK = left ? uL : uR, tK = left ? tL : tR;
         const R pK = left ? pL : pR, EK = left ? EL : ER, SK = left ? SL : SR;
         const R dK = left ? dL : dR;
-        // with dK = rK (SK - uK) and q = 1 / (SK - Ss):  fact = dK q, and
-        // fact (EK / rK + (Ss - uK)(Ss + pK / dK))
-        //   = q (EK (SK - uK) + (Ss - uK)(dK Ss + pK))   (no 1/rK, no 1/dK)
-        const R q = frcp(SK - Ss);
+        // star terms weighted by SK, or by 0 when supersonic (q forced
+        // finite), so one set of expressions gives both fluxes.  With
+        // dK = rK (SK - uK) and q = 1 / (SK - Ss):  fact = dK q, and
+        //   fact (EK / rK + (Ss - uK)(Ss + pK / dK))
+        //     = q (EK (SK - uK) + (Ss - uK)(dK Ss + pK))   (no 1/rK, no 1/dK);
+        // the tangential momentum flux is the mass flux times tK
+        const R SKw = sup ? zero : SK;
+        const R q = sup ? zero : frcp(SK - Ss);
         const R fact = dK * q;
         const R m = rK * uK;
-        const R S0 = m + SK * (fact - rK);
-        const R S1 = m * uK + pK + SK * (fact * Ss - m);
-        const R S2 = m * tK + SK * (fact * tK - rK * tK);
-        const R S3 = (EK + pK) * uK + SK * (q * (EK * (SK - uK) + (Ss - uK) * (dK * Ss + pK)) - EK);
-        // one-sided flux of the side the flow comes from when supersonic
-        const bool sup = (SL >= zero) || (SR <= zero);
-        const bool fromL = (SL >= zero);
-        const R rO = fromL ? rL : rR, uO = fromL ? uL : uR, tO = fromL ? tL : tR;
-        const R pO = fromL ? pL : pR, EO = fromL ? EL : ER;
-        const R mO = rO * uO;
-        Fh0 = sup ? mO : S0;
-        Fh1 = sup ? mO * uO + pO : S1;
-        Fh2 = sup ? mO * tO : S2;
-        Fh3 = sup ? (EO + pO) * uO : S3;
+        Fh0 = m + SKw * (fact - rK);
+        Fh1 = m * uK + pK + SKw * (fact * Ss - m);
+        Fh2 = Fh0 * tK;
+        Fh3 = (EK + pK) * uK + SKw * (q * (EK * (SK - uK) + (Ss - uK) * (dK * Ss + pK)) - EK);
     }
     // --- HLLE of the cell states, and the pressure-jump sensor ---
     R Fl0, Fl1, Fl2, Fl3, sd;
     {
         const R rL = WL[0], uL = WL[1], tL = WL[2], pL = WL[3];
         const R rR = WR[0], uR = WR[1], tR = WR[2], pR = WR[3];
-        const R SL = dmin<R>(uL - cWL, uR - cWR), SR = dmax<R>(uL + cWL, uR + cWR);
+        // Einfeldt's form: with SL- = min(SL, 0), SR+ = max(SR, 0) the HLL
+        // average equals FL, FR or the subsonic average in the three wave
+        // configurations, with no selects
+        const R SL = dmin<R>(dmin<R>(uL - cWL, uR - cWR), zero), SR = dmax<R>(dmax<R>(uL + cWL, uR + cWR), zero);
         const R mL = rL * uL, mR = rR * uR;
         const R FL1 = mL * uL + pL, FR1 = mR * uR + pR;
         const R FL2 = mL * tL, FR2 = mR * tR;
@@ -343,22 +340,16 @@ __device__ __forceinline__ void face_flux_fast(const R L[4], const R Rv[4], cons
             sd = dp2 * frcp(dd);
         }
         const R SRL = SR * SL;
-        const R H0 = (SR * mL - SL * mR + SRL * (rR - rL)) * idS;
-        const R H1 = (SR * FL1 - SL * FR1 + SRL * (mR - mL)) * idS;
-        const R H2 = (SR * FL2 - SL * FR2 + SRL * (rR * tR - rL * tL)) * idS;
-        const R H3 = (SR * FL3 - SL * FR3 + SRL * (EWR - EWL)) * idS;
-        const bool fl = (SL >= zero), fr = (SR <= zero);
-        Fl0 = fl ? mL : fr ? mR : H0;
-        Fl1 = fl ? FL1 : fr ? FR1 : H1;
-        Fl2 = fl ? FL2 : fr ? FR2 : H2;
-        Fl3 = fl ? FL3 : fr ? FR3 : H3;
+        Fl0 = (SR * mL - SL * mR + SRL * (rR - rL)) * idS;
+        Fl1 = (SR * FL1 - SL * FR1 + SRL * (mR - mL)) * idS;
+        Fl2 = (SR * FL2 - SL * FR2 + SRL * (rR * tR - rL * tL)) * idS;
+        Fl3 = (SR * FL3 - SL * FR3 + SRL * (EWR - EWL)) * idS;
     }
-    // --- Ducros blend (sd formed in the HLLE block) ---
-    const R om = R(1) - sd;
-    F[0] = om * Fh0 + sd * Fl0;
-    F[1] = om * Fh1 + sd * Fl1;
-    F[2] = om * Fh2 + sd * Fl2;
-    F[3] = om * Fh3 + sd * Fl3;
+    // --- Ducros blend: (1 - s) Fh + s Fl ---
+    F[0] = Fh0 + sd * (Fl0 - Fh0);
+    F[1] = Fh1 + sd * (Fl1 - Fh1);
+    F[2] = Fh2 + sd * (Fl2 - Fh2);
+    F[3] = Fh3 + sd * (Fl3 - Fh3);
 }
 
 }  // namespace fvb
