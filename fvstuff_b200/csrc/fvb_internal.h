@@ -90,9 +90,9 @@ struct StageArgs {
 struct TileShape {
     int tx, ty, nt;
 };
-constexpr int kNumTileShapes = 4;
+constexpr int kNumTileShapes = 6;
 constexpr TileShape kTileShapes[kNumTileShapes] = {
-    {32, 15, 256}, {32, 7, 128}, {64, 7, 256}, {16, 15, 256}};
+    {32, 15, 256}, {32, 7, 128}, {64, 7, 256}, {16, 15, 256}, {32, 9, 256}, {32, 16, 256}};
 
 // TMA descriptors (fvb_stage.cu): encode the four maps of a grid for a
 // tile shape into host memory; false if this grid cannot use TMA

@@ -73,8 +73,8 @@ __device__ __forceinline__ void face_one(const R *W, int base, R *out, int ostri
 
 // The FP64 and FP32 (reference-rounding) stage kernel, two CTAs per SM; the
 // FP32-compensated form has its own kernel (fvb_stage32c.cu).
-template <int PREC, int ORDER, int TX, int TY, int NT, bool BATCHED>
-__global__ void __launch_bounds__(NT, 2) stage_kernel(const __grid_constant__ StageArgs a)
+template <int PREC, int ORDER, int TX, int TY, int NT, bool BATCHED, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__ StageArgs a)
 {
     static_assert(PREC == P64 || PREC == P32, "FP64 and FP32 primitive-state forms");
     using R = typename PrecT<PREC>::R;
@@ -380,13 +380,14 @@ struct K {
     static constexpr TileShape ts = kTileShapes[SHAPE];
     static constexpr int G = (ORDER + 1) / 2;
     using R = typename PrecT<PREC>::R;
-    static size_t smem()
-    {
-        return sizeof(R) * (10 * (ts.ty + 2 * G) * (ts.tx + 2 * G) + 4 * ts.ty * (ts.tx + 1) +
-                            4 * (ts.ty + 1) * ts.tx);
-    }
-    static void *fn() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt, false>; }
-    static void *fn_batched() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt, true>; }
+    static constexpr size_t kSmem = sizeof(R) * (10 * (ts.ty + 2 * G) * (ts.tx + 2 * G) + 4 * ts.ty * (ts.tx + 1) +
+                                                 4 * (ts.ty + 1) * ts.tx);
+    // CTAs per SM the registers are budgeted for: three where three tiles'
+    // shared memory fits in the SM's 228 KB (1 KB reserved per CTA), else two
+    static constexpr int kMinBlocks = 3 * (kSmem + 1024) <= 228 * 1024 ? 3 : 2;
+    static size_t smem() { return kSmem; }
+    static void *fn() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt, false, kMinBlocks>; }
+    static void *fn_batched() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt, true, kMinBlocks>; }
 };
 
 struct KernelEntry {
@@ -411,7 +412,8 @@ static KernelEntry entry32c(int shape)
                        kTileShapes[shape].nt, 0, 0};
 }
 
-#define FVB_SHAPES(P, O) entry<P, O, 0>(), entry<P, O, 1>(), entry<P, O, 2>(), entry<P, O, 3>()
+#define FVB_SHAPES(P, O) \
+    entry<P, O, 0>(), entry<P, O, 1>(), entry<P, O, 2>(), entry<P, O, 3>(), entry<P, O, 4>(), entry<P, O, 5>()
 
 static KernelEntry *table_for(int prec, int order)
 {
@@ -419,7 +421,7 @@ static KernelEntry *table_for(int prec, int order)
     static KernelEntry t64_5[] = {FVB_SHAPES(P64, 5)};
     static KernelEntry t64_3[] = {FVB_SHAPES(P64, 3)};
     static KernelEntry t32_7[] = {FVB_SHAPES(P32, 7)};
-    static KernelEntry t32c_7[] = {entry32c(0), entry32c(1), entry32c(2), entry32c(3)};
+    static KernelEntry t32c_7[] = {entry32c(0), entry32c(1), entry32c(2), entry32c(3), entry32c(4), entry32c(5)};
     if (prec == P64) return order == 7 ? t64_7 : order == 5 ? t64_5 : order == 3 ? t64_3 : nullptr;
     if (order != 7) return nullptr;
     return prec == P32 ? t32_7 : prec == P32C ? t32c_7 : nullptr;

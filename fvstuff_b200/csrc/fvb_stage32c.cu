@@ -326,6 +326,8 @@ void *stage32c_fn(int shape, bool batched)
     case 1: return fn32c<1>(batched);
     case 2: return fn32c<2>(batched);
     case 3: return fn32c<3>(batched);
+    case 4: return fn32c<4>(batched);
+    case 5: return fn32c<5>(batched);
     default: return nullptr;
     }
 }

@@ -57,6 +57,18 @@ def test_f32c_kh_short_against_f64():
     assert e[0] <= 1e-6
 
 
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
+def test_f32c_tile_variants_against_f64(tile):
+    """Every tile variant of the compensated kernel, on a ragged grid with
+    reflecting walls (ghost images with negated momenta on all four sides)."""
+    n, steps = 77, 40
+    w = vortex(n)
+    kw = dict(bc="reflect", x0=-5, y0=-5, length=10.0, cfl=0.5)
+    _, c64, _ = _run("f64", w, steps, **kw)
+    _, c32, _ = _run("f32c", w, steps, tile=tile, **kw)
+    assert rel_l1(c32[0], c64[0]) <= 1e-6
+
+
 def test_f32c_hilo_is_normalised_and_conservative():
     n = 64
     s = F.Solver(n, precision="f32c", bc="periodic")

@@ -158,7 +158,7 @@ def test_step_f64_matches_oracle(bc, n, case):
     assert rel_linf(got, ref) <= TOL64
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2, 3])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
 def test_tile_variants_agree(tile):
     n = 70
     U = _padded(riemann4(n, seed=5), 1)
