@@ -212,6 +212,23 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         }
         const R dt = R(ctl.dt);
         const R inv_h = R(1.0 / gd.h);
+        // U0 of this thread's cells (stages 2 and 3), loaded now so the loads
+        // are in flight while the faces are computed
+        constexpr int CPT = (TX * TY + NT - 1) / NT;  // cells per thread
+        static_assert(CPT <= 2, "at most two cells a thread");
+        R u0v[CPT][4];
+        if (a.stage >= 2) {
+            const R *u0 = (const R *)gd.st[0];
+#pragma unroll
+            for (int it = 0; it < CPT; ++it) {
+                const int k = tid + it * NT, r = k / TX, c = k - r * TX, i = tx0 + c, j = ty0 + r;
+                if (k < TX * TY && i < n && j < n) {
+                    const long long e = gidx(gd, 0, j, i);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) u0v[it][q] = u0[e + q * gd.plane];
+                }
+            }
+        }
 
         // ---- 3. face fluxes: x-faces, then y-faces (compile-time strides) ---
         for (int f = tid; f < NXF; f += NT) {
@@ -228,7 +245,10 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
 
         // ---- 4. divergence, RK combination, stores ------------------------
         double lmax = 0.0;
-        for (int k = tid; k < TX * TY; k += NT) {
+#pragma unroll
+        for (int it = 0; it < CPT; ++it) {
+            const int k = tid + it * NT;
+            if (k >= TX * TY) break;
             int r = k / TX, c = k - r * TX, i = tx0 + c, j = ty0 + r;
             if (i >= n || j >= n) continue;
             R res[4];
@@ -255,10 +275,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
 #pragma unroll
                     for (int q = 0; q < 4; ++q) w0[q] = wk[q];
                 } else {
-                    const R *u0 = (const R *)gd.st[0];
-                    const long long e = gidx(gd, 0, j, i);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) w0[q] = u0[e + q * gd.plane];
+                    for (int q = 0; q < 4; ++q) w0[q] = u0v[it][q];
                 }
                 if constexpr (FAST) {
                     c0[0] = w0[0]; c0[1] = w0[0] * w0[1]; c0[2] = w0[0] * w0[2];
