@@ -32,6 +32,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from fvstuff_b200 import ranks as R  # noqa: E402  (no torch / CUDA at import)
+
 BYTES_PER_CELL_STAGE = {"f64": 256.0 / 3.0, "f32": 128.0 / 3.0, "f32c": 160.0 / 3.0}
 METRIC = "cell-stage updates/s on 1 B200 (plain vs batched/served); p50/p99 solve latency"
 
@@ -212,14 +214,6 @@ def measure_form(F, torch, stream, precision, n, steps, warmup, dist):
     return s, ms
 
 
-def max_over_ranks(torch, dist, x):
-    if not dist:
-        return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
 def e2e_run(F, torch, stream, precision, n, steps, dist):
     """Through the public API with host buffers: upload the initial state from
     pinned host memory, then per step one fvb_step and one fvb_sync (the D2H
@@ -242,7 +236,7 @@ def e2e_run(F, torch, stream, precision, n, steps, dist):
         s.sync()
     s.get_state(interior=True, out=host_out.numpy())
     t1 = time.perf_counter()
-    sec = max_over_ranks(torch, dist, t1 - t0)
+    sec = R.max_over_ranks(t1 - t0, dist)
     s.close()
     state_bytes = 4 * n * n * 8
     return sec, state_bytes / steps + 8, state_bytes / steps + 80
@@ -253,24 +247,16 @@ def run_gpu(args):
 
     import fvstuff_b200 as F
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = R.env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as D
-        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        dist = D
+    dist = R.init("nccl")
     stream = torch.cuda.Stream()
     n, K, W = args.n, args.steps, args.warmup
     hbm, peak_kind = peaks()
 
     with ClockSampler(local) as clk:
         s, ms = measure_form(F, torch, stream, args.precision, n, K, W, dist)
-    ms = max_over_ranks(torch, dist, ms)
+    ms = R.max_over_ranks(ms, dist)
     s.close()
     units = 3.0 * n * n * K
     value = world * units / (ms / 1e3)
@@ -293,7 +279,7 @@ def run_gpu(args):
         with ClockSampler(local):
             s2, ms2 = measure_form(F, torch, stream, "f32c", n, K, W, dist)
         s2.close()
-        ms2 = max_over_ranks(torch, dist, ms2)
+        ms2 = R.max_over_ranks(ms2, dist)
         v2 = world * units / (ms2 / 1e3)
         a2 = BYTES_PER_CELL_STAGE["f32c"] * n * n / (ms2 / (3 * K) / 1e3) / 1e9
         line["forms"] = {"f32c": {"value": v2, "ms_per_step": ms2 / K, "vs_f64": v2 / value,
@@ -310,9 +296,7 @@ def run_gpu(args):
         rate, kind, threads, sec = cpu_reference_rate(min(n, 512), 4, 1)
         line["cpu_baseline"] = {"value": rate, "unit": "cell-stage updates/s", "cores": threads, "kind": kind,
                                 "sample": "4 SSP-RK3 steps of the KH case on a %dx%d grid" % ((min(n, 512),) * 2)}
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    R.finish(dist)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -370,14 +354,21 @@ def run_batched(args):
     import torch
 
     import fvstuff_b200 as F
+    rank, world, local = R.env()
+    torch.cuda.set_device(local)
+    dist = R.init("nccl")
     count = args.instances
     insts = riemann_instances(count)
+    # N ranks split the instances by work (~N^3: cells x steps)
+    mine = [insts[i] for i in R.shard_by_work([float(n) ** 3 for n, _ in insts], rank, world)]
     t_end = 0.25
     b = F.Batch(precision="f32c")
     ids = {}
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
-    for n, c in insts:
+    for n, c in mine:
         ids[b.add(F.Batch.desc(n, c, t_end, bc="transmissive", cfl=0.5))] = n
     done = set()
     while len(done) < len(ids):
@@ -390,17 +381,27 @@ def run_batched(args):
         bad += st.status != 0
         work += 3.0 * n * n * st.steps
     b.close()
+    sec = R.max_over_ranks(sec, dist)
+    work = R.sum_over_ranks(work, dist)
+    bad = int(R.sum_over_ranks(bad, dist))
     value = work / sec
-    # the plain FP64 form on the same grids one at a time: a seeded sample of
-    # them, the rate scaled to the sample's own work
+    # the plain FP64 form on the same grids one at a time (per GPU): a seeded
+    # sample of them, the rate scaled to the sample's own work
     sample = insts[:: max(1, count // args.plain_sample)]
-    pw, ps, pbad = run_plain_f64_alone(F, sample, t_end)
-    line = {"metric": METRIC, "value": value, "unit": "cell-stage updates/s", "n_gpus": 1, "steps": None,
-            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
+    my_sample = [sample[i] for i in R.shard_by_work([float(n) ** 3 for n, _ in sample], rank, world)]
+    pw, ps, pbad = run_plain_f64_alone(F, my_sample, t_end)
+    pw = R.sum_over_ranks(pw, dist)
+    ps = R.max_over_ranks(ps, dist)
+    pbad = int(R.sum_over_ranks(pbad, dist))
+    R.finish(dist)
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": "cell-stage updates/s", "n_gpus": world, "steps": None,
+            "warmup": 0, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32c",
             "data": "synthetic", "mode": "batched",
             "config": {"workload": "%d four-quadrant Riemann problems, N in {64..512} step 32, transmissive, "
                                    "t=0.25, CFL 0.5, one persistent launch per RK stage (graph-replayed)" % count,
-                       "instances": count,
+                       "instances": count, "parallelism": "instances split by work over %d GPU(s)" % world,
                        "failed": bad, "failed_means": "stopped by the blow-up / dt-underflow guard of the "
                                                      "reference scheme before t_end; their steps count"},
             "seconds": sec, "cell_stages": work,
@@ -410,15 +411,15 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
-def run_serve(args):
-    import torch
-
-    import fvstuff_b200 as F
+def serve_requests(F, count, rate, max_n):
+    """The seeded request stream: Poisson arrivals, half isentropic vortices
+    (periodic [-5,5]^2), half four-quadrant Riemann problems (transmissive
+    [0,1]^2), N log-uniform in [128, max_n], t_end uniform in [0.1, 1]."""
     rng = np.random.default_rng(7)
     reqs, t = [], 0.0
-    for k in range(args.requests):
-        t += rng.exponential(1.0 / args.rate)
-        n = int(round(math.exp(rng.uniform(math.log(128), math.log(args.max_n)))))
+    for k in range(count):
+        t += rng.exponential(1.0 / rate)
+        n = int(round(math.exp(rng.uniform(math.log(128), math.log(max_n)))))
         t_end = float(rng.uniform(0.1, 1.0))
         if rng.random() < 0.5:
             c = F.case_params("vortex", -5.0, -5.0, 10.0)
@@ -427,14 +428,30 @@ def run_serve(args):
             c = F.case_params("riemann4", 0.0, 0.0, 1.0, seed=int(rng.integers(1, 2 ** 62)))
             d = F.Batch.desc(n, c, t_end, bc="transmissive", cfl=0.5)
         reqs.append((t, d))
+    return reqs
+
+
+def run_serve(args):
+    import torch
+
+    import fvstuff_b200 as F
+    rank, world, local = R.env()
+    torch.cuda.set_device(local)
+    dist = R.init("nccl")
+    reqs = serve_requests(F, args.requests, args.rate, args.max_n)
+    # N ranks: request k goes to rank k mod N, each rank serves its own stream
+    mine = reqs[rank::world]
     torch.cuda.synchronize()
-    res, wall = F.serve_run(reqs, precision="f32c", hbm_budget=150 << 30, steps_per_round=args.steps_per_round)
-    lat = sorted(r["finished"] - r["arrival"] for r in res)
-    work = sum(3.0 * d.n * d.n * r["steps"] for (_, d), r in zip(reqs, res))
+    if dist:
+        dist.barrier()
+    res, wall = F.serve_run(mine, precision="f32c", hbm_budget=150 << 30, steps_per_round=args.steps_per_round)
+    lat = [r["finished"] - r["arrival"] for r in res]
+    work = sum(3.0 * d.n * d.n * r["steps"] for (_, d), r in zip(mine, res))
+    failed = sum(r["status"] != 0 for r in res)
     # the same requests one at a time on the plain FP64 path, back to back
     t0 = time.perf_counter()
     seq_lat, clock = [], 0.0
-    for (arr, d), r in zip(reqs, res):
+    for (arr, d), r in zip(mine, res):
         s = F.Solver(d.n, bc={0: "reflect", 1: "periodic", 2: "transmissive"}[d.bc_x], x0=d.x0, y0=d.y0,
                      length=d.length, cfl=d.cfl, precision="f64")
         s.init_case(d.ic)
@@ -444,16 +461,25 @@ def run_serve(args):
         seq_lat.append(clock - arr)
         s.close()
     seq_wall = time.perf_counter() - t0
-    seq_lat.sort()
+    lat = sorted(sum(R.gather(lat, dist), []))
+    seq_lat = sorted(sum(R.gather(seq_lat, dist), []))
+    wall = R.max_over_ranks(wall, dist)
+    seq_wall = R.max_over_ranks(seq_wall, dist)
+    work = R.sum_over_ranks(work, dist)
+    failed = int(R.sum_over_ranks(failed, dist))
+    R.finish(dist)
+    if rank != 0:
+        return
     pct = lambda v, q: v[min(len(v) - 1, int(q * len(v)))]
-    line = {"metric": METRIC, "value": work / wall, "unit": "cell-stage updates/s", "n_gpus": 1,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32c", "data": "synthetic",
+    line = {"metric": METRIC, "value": work / wall, "unit": "cell-stage updates/s", "n_gpus": world,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32c", "data": "synthetic",
             "mode": "serve",
             "config": {"workload": "Poisson stream, %d requests at %.0f/s, vortex or seeded Riemann, N log-uniform "
                                    "in [128, %d], t_end U[0.1, 1], 150 GB HBM budget" % (args.requests, args.rate,
-                                                                                        args.max_n)},
+                                                                                        args.max_n),
+                       "parallelism": "request k served by GPU k mod %d" % world},
             "p50_s": pct(lat, 0.5), "p99_s": pct(lat, 0.99), "wall_s": wall,
-            "failed": sum(r["status"] != 0 for r in res),
+            "failed": failed,
             "sequential_plain_f64": {"value": work / seq_wall, "p50_s": pct(seq_lat, 0.5),
                                      "p99_s": pct(seq_lat, 0.99), "wall_s": seq_wall}}
     print(json.dumps(line), flush=True)
