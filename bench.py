@@ -133,7 +133,8 @@ def peaks():
 
 def traffic_from_profiles(precision: str, n: int):
     """dram bytes per stage launch from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / ("stage_kernel_kh%d_%s.txt" % (n, precision))
+    kernel = "stage32c_kernel" if precision == "f32c" else "stage_kernel"
+    f = ROOT / "profiles" / ("%s_kh%d_%s.txt" % (kernel, n, precision))
     if not f.exists():
         return None
     for line in f.read_text().splitlines():

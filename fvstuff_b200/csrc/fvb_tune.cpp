@@ -3,10 +3,12 @@
 //
 // On first use for a (device, precision, order, grid-size class) the tuner
 // builds a scratch grid of a representative size (the grid's own size, at
-// most 1024^2), fills it with a smooth state, and times a few SSP-RK3 steps
+// most 2048^2), fills it with a smooth state, and times a few SSP-RK3 steps
 // of every tile variant that can be resident on the device with CUDA
 // events; the fastest wins and is cached for the process.  FVB_TILE=<k>
-// forces variant k; FVB_AUTOTUNE=0 selects variant 0 without measuring.
+// forces variant k; FVB_AUTOTUNE=0 selects variant 0 without measuring;
+// FVB_AUTOTUNE_LOG=1 prints each variant's time and the choice to stderr.
+#include <cstdio>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -92,11 +94,20 @@ float time_shape(int prec, int order, int n, int shape, cudaStream_t s)
         if (!run(2)) break;  // warm-up (even: F32C ends on its start buffer)
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
-        cudaEventRecord(e0, s);
-        if (!run(4)) break;
-        cudaEventRecord(e1, s);
-        if (cudaEventSynchronize(e1) != cudaSuccess) break;
-        cudaEventElapsedTime(&ms, e0, e1);
+        // the best of three timings of four steps: variants differ by a few
+        // per cent, about the run-to-run spread of a single timing
+        bool ok = true;
+        for (int rep = 0; rep < 3 && ok; ++rep) {
+            cudaEventRecord(e0, s);
+            ok = run(4);
+            cudaEventRecord(e1, s);
+            float t = -1.f;
+            if (ok && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess)
+                ms = (ms < 0.f || t < ms) ? t : ms;
+            else
+                ok = false;
+        }
+        if (!ok) ms = -1.f;
     } while (0);
     cudaStreamSynchronize(s);
     if (e0) cudaEventDestroy(e0);
@@ -125,16 +136,22 @@ int autotune_shape(int prec, int order, int n)
     if (it != g_cache.end()) return it->second;
     cudaStream_t s = nullptr;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return 0;
-    const int nt = n < 1024 ? (n < 16 ? 16 : n) : 1024;
+    const int nt = n < 2048 ? (n < 16 ? 16 : n) : 2048;
     int best = 0;
     float best_ms = -1.f;
+    const bool log = std::getenv("FVB_AUTOTUNE_LOG") != nullptr;
     for (int shape = 0; shape < kNumTileShapes; ++shape) {
         float ms = time_shape(prec, order, nt, shape, s);
+        if (log)
+            std::fprintf(stderr, "fvb autotune: precision %d order %d n %d: tile %d (%dx%d, %d threads) %.4f ms\n",
+                         prec, order, nt, shape, kTileShapes[shape].tx, kTileShapes[shape].ty, kTileShapes[shape].nt,
+                         ms);
         if (ms > 0 && (best_ms < 0 || ms < best_ms)) {
             best_ms = ms;
             best = shape;
         }
     }
+    if (log) std::fprintf(stderr, "fvb autotune: -> tile %d\n", best);
     cudaStreamDestroy(s);
     g_cache[key] = best;
     return best;
