@@ -173,6 +173,21 @@ class Solver:
         check(lib().fvb_get_state_hilo(self._h, hi.ctypes.data, lo.ctypes.data), "fvb_get_state_hilo")
         return hi, lo
 
+    # frames ------------------------------------------------------------------
+    FRAME_FIELDS = ("rho", "vorticity", "ducros", "speed", "p")
+
+    def frame_begin(self) -> None:
+        """Start extracting fv_up7's frame fields from the current state (on
+        the device; copied to host on a second stream).  Steps enqueued after
+        this call overlap the copy."""
+        check(lib().fvb_frame_begin(self._h), "fvb_frame_begin")
+
+    def frame_end(self) -> dict:
+        """Wait for the frame begun last; {field: (n, n) float32 array}."""
+        out = np.empty((5, self.n, self.n), np.float32)
+        check(lib().fvb_frame_end(self._h, out.ctypes.data), "fvb_frame_end")
+        return dict(zip(self.FRAME_FIELDS, out))
+
     # stepping ----------------------------------------------------------------
     def step(self, nsteps: int = 1, t_stop: float = math.inf) -> None:
         """Enqueue up to `nsteps` steps (asynchronous)."""

@@ -72,72 +72,52 @@ Args parse(int argc, char **argv)
     return a;
 }
 
+// Frame fields come from the device (fvb_frame_begin / fvb_frame_end):
+// density, vorticity, Ducros cell sensor, |v|, pressure.  A frame is begun
+// right after the steps that reach its time, the next steps are enqueued,
+// and only then is it collected and written, so the image work on the host
+// overlaps the GPU's next steps.
 struct Frames {
-    int N, g, Np;
-    double h;
-    float rho_lo, rho_hi;
-    std::vector<float> Q, rho, p, sd, vort, vmag;
-    explicit Frames(int n, int gg, double hh) : N(n), g(gg), Np(n + 2 * gg), h(hh)
-    {
-        Q.resize((size_t)4 * Np * Np);
-        for (auto *v : {&rho, &p, &sd, &vort, &vmag}) v->resize((size_t)N * N);
-    }
-    float at(int q, int jp, int ip) const { return Q[(size_t)q * Np * Np + (size_t)jp * Np + ip]; }
-    // Ducros cell sensor (max of its 4 faces), 6th-order vorticity and |v|
-    //                                   fv_up7_ducros_2d.cu:511-526, :800-829
-    void derive()
-    {
-        auto ducros = [](float pa, float pb) {
-            float dp = pb - pa, ps = pb + pa;
-            return dp * dp / (dp * dp + 0.1f * ps * ps);
-        };
-        static const float coeff[6] = {-1.f, 9.f, -45.f, 45.f, -9.f, 1.f};
-        static const int off[6] = {-3, -2, -1, 1, 2, 3};
-        for (int j = 0; j < N; ++j)
-            for (int i = 0; i < N; ++i) {
-                const int jp = j + g, ip = i + g;
-                const size_t k = (size_t)j * N + i;
-                rho[k] = at(0, jp, ip);
-                p[k] = at(3, jp, ip);
-                sd[k] = std::fmax(std::fmax(ducros(at(3, jp, ip), at(3, jp, ip + 1)), ducros(at(3, jp, ip - 1), at(3, jp, ip))),
-                                  std::fmax(ducros(at(3, jp, ip), at(3, jp + 1, ip)), ducros(at(3, jp - 1, ip), at(3, jp, ip))));
-                float dvdx = 0.f, dudy = 0.f;
-                for (int d = 0; d < 6; ++d) {
-                    if (g >= 3) {
-                        dvdx += coeff[d] * at(2, jp, ip + off[d]);
-                        dudy += coeff[d] * at(1, jp + off[d], ip);
-                    }
-                }
-                vort[k] = (dvdx - dudy) / (60.0f * (float)h);
-                const float u = at(1, jp, ip), v = at(2, jp, ip);
-                vmag[k] = std::sqrt(u * u + v * v);
-            }
-    }
+    int N;
+    float rho_lo = 0.f, rho_hi = 1.f;
+    std::vector<float> buf;  // 5 x N x N
+    explicit Frames(int n) : N(n), buf((size_t)5 * n * n) {}
+    const float *field(int k) const { return buf.data() + (size_t)k * N * N; }
 };
 
-bool write_frame(fvb_solver *s, Frames &F, const Args &a, int idx)
+bool finish_frame(fvb_solver *s, Frames &F, const Args &a, int idx)
 {
-    if (fvb_get_state(s, F.Q.data(), FVB_LAYOUT_PRIM, FVB_F32, FVB_HOST, 0)) {
-        std::fprintf(stderr, "state read failed: %s\n", fvb_last_error());
+    if (fvb_frame_end(s, F.buf.data())) {
+        std::fprintf(stderr, "frame read failed: %s\n", fvb_last_error());
         return false;
     }
-    F.derive();
+    const size_t nn = (size_t)F.N * F.N;
+    const float *rho = F.field(0), *vort = F.field(1), *sd = F.field(2), *vmag = F.field(3), *p = F.field(4);
     char fn[512];
     if (a.ppm) {
         float wmax = 1e-10f, vmax = 1e-10f;
-        for (size_t k = 0; k < F.vort.size(); ++k) {
-            wmax = std::max(wmax, std::fabs(F.vort[k]));
-            vmax = std::max(vmax, F.vmag[k]);
+        for (size_t k = 0; k < nn; ++k) {
+            wmax = std::max(wmax, std::fabs(vort[k]));
+            vmax = std::max(vmax, vmag[k]);
         }
         std::snprintf(fn, sizeof fn, "%s_%04d.ppm", a.prefix.c_str(), idx);
-        fvbio::write_ppm_2x2(fn, {F.rho.data(), F.rho_lo, F.rho_hi, fvbio::PLASMA}, {F.vort.data(), -wmax, wmax, fvbio::BWR},
-                             {F.sd.data(), 0.f, 1.f, fvbio::HOT}, {F.vmag.data(), 0.f, vmax, fvbio::VIRIDIS}, F.N);
+        fvbio::write_ppm_2x2(fn, {rho, F.rho_lo, F.rho_hi, fvbio::PLASMA}, {vort, -wmax, wmax, fvbio::BWR},
+                             {sd, 0.f, 1.f, fvbio::HOT}, {vmag, 0.f, vmax, fvbio::VIRIDIS}, F.N);
     }
     if (a.bin) {
         std::snprintf(fn, sizeof fn, "%s_%04d.bin", a.prefix.c_str(), idx);
-        fvbio::write_bin(fn, F.rho.data(), F.p.data(), F.N);
+        fvbio::write_bin(fn, rho, p, F.N);
     }
     return true;
+}
+
+bool write_frame_now(fvb_solver *s, Frames &F, const Args &a, int idx)
+{
+    if (fvb_frame_begin(s)) {
+        std::fprintf(stderr, "frame: %s\n", fvb_last_error());
+        return false;
+    }
+    return finish_frame(s, F, a, idx);
 }
 
 }  // namespace
@@ -168,14 +148,16 @@ int main(int argc, char **argv)
     fvb_case_default(&c, a.kase, cfg.x0, cfg.y0, cfg.length);
     if (a.seed >= 0) c.seed = (uint64_t)a.seed;
     if (fvb_init_case(s, &c)) { std::fprintf(stderr, "init: %s\n", fvb_last_error()); return 1; }
-    Frames F(a.n, g, h);
+    Frames F(a.n);
     // density colour scale fixed to the initial extremes for the whole run
     // (the reference fixes 0.125 .. 10.1 for its Sod case, :932)
     if (a.kase == FVB_CASE_SOD) { F.rho_lo = 0.125f; F.rho_hi = 10.1f; }
     else {
-        fvb_get_state(s, F.Q.data(), FVB_LAYOUT_PRIM, FVB_F32, FVB_HOST, 0);
-        F.derive();
-        auto mm = std::minmax_element(F.rho.begin(), F.rho.end());
+        if (fvb_frame_begin(s) || fvb_frame_end(s, F.buf.data())) {
+            std::fprintf(stderr, "frame: %s\n", fvb_last_error());
+            return 1;
+        }
+        auto mm = std::minmax_element(F.field(0), F.field(0) + (size_t)a.n * a.n);
         F.rho_lo = *mm.first; F.rho_hi = *mm.second;
     }
     if (!a.resume.empty()) {
@@ -184,31 +166,42 @@ int main(int argc, char **argv)
     fvb_stats st;
     fvb_sync(s, &st);
     int frame = 1;
-    if (a.resume.empty() || st.t == 0.0) write_frame(s, F, a, 0);
+    if (a.resume.empty() || st.t == 0.0) write_frame_now(s, F, a, 0);
     else while (frame <= a.frames && st.t >= frame * a.t_end / a.frames - 1e-12) ++frame;
     double t_next = frame * a.t_end / a.frames;
     const auto t0 = std::chrono::steady_clock::now();
     auto elapsed = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
     long long last_print = st.steps;
+    bool enqueued = false;  // steps already on the stream (issued behind a frame)
+    // at most 50 steps per call so progress prints like the reference's
+    auto issue = [&](const fvb_stats &cur) {
+        const int chunk = (int)(50 - (cur.steps % 50));
+        return fvb_step(s, chunk, std::min(t_next, a.t_end)) == FVB_OK;
+    };
     while (st.t < a.t_end) {
-        const double target = std::min(t_next, a.t_end);
-        // at most 50 steps per call so progress prints like the reference's
-        int chunk = (int)(50 - (st.steps % 50));
-        if (fvb_step(s, chunk, target) || fvb_sync(s, &st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }
+        if (!enqueued && !issue(st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }
+        enqueued = false;
+        if (fvb_sync(s, &st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }
         if (st.status) {
             std::fprintf(stderr, "  %s at step %lld t=%.6f lam_max=%.3e -- writing blow-up frame\n",
                          st.status == FVB_ERR_BLOWUP ? "NaN/Inf lam_max" : "dt underflow", (long long)st.steps, st.t,
                          st.lam_max);
-            write_frame(s, F, a, 99);
+            write_frame_now(s, F, a, 99);
             break;
         }
         if (st.t >= t_next - 1e-12 && frame <= a.frames) {
             std::printf("  frame %2d/%d  step %5lld  t=%.5f  elapsed=%.1fs\n", frame, a.frames, (long long)st.steps,
                         st.t, elapsed());
             std::fflush(stdout);
-            write_frame(s, F, a, frame);
+            if (fvb_frame_begin(s)) { std::fprintf(stderr, "frame: %s\n", fvb_last_error()); return 1; }
             ++frame;
             t_next = frame * a.t_end / a.frames;
+            // the next steps run on the GPU while this frame is written
+            if (st.t < a.t_end) {
+                if (!issue(st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }
+                enqueued = true;
+            }
+            finish_frame(s, F, a, frame - 1);
         } else if (st.steps / 50 != last_print / 50) {
             const double el = elapsed();
             std::printf("  step %5lld  t=%.5f  dt=%.3e  elapsed=%.1fs  ETA=%.0fs\n", (long long)st.steps, st.t, st.dt,

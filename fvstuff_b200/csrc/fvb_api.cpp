@@ -143,6 +143,13 @@ struct fvb_solver {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int graph_steps = 1;
     bool keep = false;  // KEEP flux family: conserved FP64 state, g = 2
+    // frame extraction (fvb_frame_begin / fvb_frame_end)
+    float *frame_prim = nullptr;   // device, FP32 primitives with ghosts
+    float *frame_dev = nullptr;    // device, 5 n x n fields
+    float *frame_host = nullptr;   // pinned copy of them
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t frame_ready = nullptr, frame_copied = nullptr;
+    bool frame_pending = false, frame_used = false;
 };
 
 static fvb_status ensure_staging(fvb_solver *s)
@@ -392,6 +399,13 @@ void fvb_destroy(fvb_solver *s)
     if (s->sums_dev) cudaFree(s->sums_dev);
     if (s->sums_host) cudaFreeHost(s->sums_host);
     if (s->ctrl_host) cudaFreeHost(s->ctrl_host);
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
+    if (s->frame_prim) cudaFree(s->frame_prim);
+    if (s->frame_dev) cudaFree(s->frame_dev);
+    if (s->frame_host) cudaFreeHost(s->frame_host);
+    if (s->frame_ready) cudaEventDestroy(s->frame_ready);
+    if (s->frame_copied) cudaEventDestroy(s->frame_copied);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -467,6 +481,52 @@ fvb_status fvb_get_state(fvb_solver *s, void *dst, int layout, int dtype, int wh
         e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess) return cuda_fail(e, "sync");
     }
+    return FVB_OK;
+}
+
+// ---- frames: extraction on the device, copy on a second stream ----------
+
+fvb_status fvb_frame_begin(fvb_solver *s)
+{
+    if (!s) return fail(FVB_ERR_INVALID, "null argument");
+    const size_t n2 = (size_t)s->n * s->n, np2 = (size_t)s->G.np * s->G.np;
+    cudaError_t e = cudaSuccess;
+    if (!s->frame_dev) {
+        e = cudaMalloc(&s->frame_prim, 4 * np2 * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&s->frame_dev, 5 * n2 * sizeof(float));
+        if (e == cudaSuccess) e = cudaMallocHost(&s->frame_host, 5 * n2 * sizeof(float));
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->frame_ready, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->frame_copied, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(e, "frame buffers");
+    }
+    // the previous frame's copy must be done before its buffers are reused
+    if (s->frame_used) e = cudaStreamWaitEvent(s->stream, s->frame_copied, 0);
+    ExtView ev{0, s->g, s->G.np, FVB_LAYOUT_PRIM, FVB_F32};
+    const int p = s->parity;
+    if (e == cudaSuccess)
+        e = export_state(s->gd.st[s->internal == INT_CONS_HILO ? p : 0], s->gd.lo[p], view_of(s->gd), s->internal,
+                         s->frame_prim, ev, s->cfg.gamma, s->stream);
+    if (e == cudaSuccess) e = frame_fields(s->frame_prim, s->n, s->g, s->G.np, s->gd.h, s->frame_dev, s->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(s->frame_ready, s->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copy_stream, s->frame_ready, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->frame_host, s->frame_dev, 5 * n2 * sizeof(float), cudaMemcpyDeviceToHost,
+                            s->copy_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(s->frame_copied, s->copy_stream);
+    if (e != cudaSuccess) return cuda_fail(e, "frame");
+    s->frame_pending = s->frame_used = true;
+    return FVB_OK;
+}
+
+fvb_status fvb_frame_end(fvb_solver *s, float *out)
+{
+    if (!s || !out) return fail(FVB_ERR_INVALID, "null argument");
+    if (!s->frame_pending) return fail(FVB_ERR_INVALID, "no frame begun");
+    cudaError_t e = cudaEventSynchronize(s->frame_copied);
+    if (e != cudaSuccess) return cuda_fail(e, "frame copy");
+    std::memcpy(out, s->frame_host, (size_t)5 * s->n * s->n * sizeof(float));
+    s->frame_pending = false;
     return FVB_OK;
 }
 

@@ -524,4 +524,53 @@ cudaError_t ctrl_set(Ctrl *c, double t_stop, int reset, double t0, double cfl, d
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// frame fields of fv_up7's composite image, from an FP32 primitive IDX_P
+// array with its ghost ring: density, 6th-order vorticity (dv/dx - du/dy,
+// central differences over +-3 cells; 0 when the ghost ring is narrower),
+// the Ducros cell sensor (max over the cell's four faces of
+// dp^2 / (dp^2 + 0.1 (pa + pb)^2)), |v| and pressure.  Output: 5 planes of
+// n x n floats, row-major, j = 0 at the bottom.
+//                                  fv_up7_ducros_2d.cu:114-133, :511-526, :800-829
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float frame_ducros(float pa, float pb)
+{
+    const float dp = pb - pa, ps = pb + pa;
+    return dp * dp / (dp * dp + 0.1f * ps * ps);
+}
+
+__global__ void frame_kernel(const float *Q, int n, int g, int np, float h, float *out)
+{
+    const long long nn = (long long)n * n;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn; k += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(k / n), i = (int)(k - (long long)j * n);
+        const long long pl = (long long)np * np;
+        auto at = [&](int q, int jp, int ip) { return Q[q * pl + (long long)jp * np + ip]; };
+        const int jp = j + g, ip = i + g;
+        const float p = at(3, jp, ip);
+        const float sx = fmaxf(frame_ducros(p, at(3, jp, ip + 1)), frame_ducros(at(3, jp, ip - 1), p));
+        const float sy = fmaxf(frame_ducros(p, at(3, jp + 1, ip)), frame_ducros(at(3, jp - 1, ip), p));
+        float w = 0.0f;
+        if (g >= 3) {
+            const float dvdx = -at(2, jp, ip - 3) + 9.0f * at(2, jp, ip - 2) - 45.0f * at(2, jp, ip - 1) +
+                               45.0f * at(2, jp, ip + 1) - 9.0f * at(2, jp, ip + 2) + at(2, jp, ip + 3);
+            const float dudy = -at(1, jp - 3, ip) + 9.0f * at(1, jp - 2, ip) - 45.0f * at(1, jp - 1, ip) +
+                               45.0f * at(1, jp + 1, ip) - 9.0f * at(1, jp + 2, ip) + at(1, jp + 3, ip);
+            w = (dvdx - dudy) / (60.0f * h);
+        }
+        const float u = at(1, jp, ip), v = at(2, jp, ip);
+        out[k] = at(0, jp, ip);
+        out[nn + k] = w;
+        out[2 * nn + k] = fmaxf(sx, sy);
+        out[3 * nn + k] = sqrtf(u * u + v * v);
+        out[4 * nn + k] = p;
+    }
+}
+
+cudaError_t frame_fields(const float *prim, int n, int g, int np, double h, float *out, cudaStream_t s)
+{
+    frame_kernel<<<592, 256, 0, s>>>(prim, n, g, np, (float)h, out);
+    return cudaGetLastError();
+}
+
 }  // namespace fvb

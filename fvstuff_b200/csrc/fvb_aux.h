@@ -39,5 +39,8 @@ cudaError_t rk3_stage_ref(int stage, R *Uo, const R *U0, const R *Uk, const R *L
                           double gam, cudaStream_t s);
 cudaError_t max_ref(const void *x, size_t n, void *out, int dtype, cudaStream_t s);
 cudaError_t ctrl_set(Ctrl *c, double t_stop, int reset, double t0, double cfl, double h, cudaStream_t s);
+// rho, vorticity, Ducros cell sensor, |v|, p (5 x n x n floats) from an FP32
+// primitive IDX_P array with its ghost ring
+cudaError_t frame_fields(const float *prim, int n, int g, int np, double h, float *out, cudaStream_t s);
 
 }  // namespace fvb

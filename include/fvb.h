@@ -147,6 +147,18 @@ FVB_API fvb_status fvb_get_state(fvb_solver *s, void *dst, int layout, int dtype
 /* hi/lo words of the compensated state, conserved, interior, FP32 each */
 FVB_API fvb_status fvb_get_state_hilo(fvb_solver *s, float *hi, float *lo);
 
+/* Frame fields of fv_up7's composite image (fv_up7_ducros_2d.cu:800-829,
+ * :511-526), extracted on the device from the state as it stands after the
+ * steps already enqueued: density, 6th-order vorticity, the Ducros cell
+ * sensor, |v| and pressure, 5 planes of N x N floats (row-major, j = 0 at the
+ * bottom).  fvb_frame_begin enqueues the extraction on the solver's stream and
+ * the copy to host on a second stream, and returns; steps enqueued after it
+ * run while the frame is copied and written.  fvb_frame_end waits for that
+ * copy and writes the 5 N N floats to `out`.  The reference computes these on
+ * the host after a blocking copy of the whole state. */
+FVB_API fvb_status fvb_frame_begin(fvb_solver *s);
+FVB_API fvb_status fvb_frame_end(fvb_solver *s, float *out);
+
 /* Checkpoint / resume: the exact internal state (every padded buffer word),
  * the time, the step count and the wave-speed max that sets the next dt, so
  * a resumed run continues bit for bit.  The reference writes images only

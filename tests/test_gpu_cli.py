@@ -1,6 +1,7 @@
 """Command-line drop-ins and outputs on the GPU: fvb_up7 (fv_up7's CLI,
 composite PPM frames, raw .bin frames, frame 99 on blow-up) and fvb_keep
-(keep_fv's CLI, 2-panel PNG), and exact checkpoint / resume."""
+(keep_fv's CLI, 2-panel PNG), the device-side frame fields, and exact
+checkpoint / resume."""
 from __future__ import annotations
 
 import struct
@@ -108,3 +109,40 @@ def test_fvb_keep_lmv(tmp_path):
     for k in range(11):
         w, h = _png(tmp_path / "figures" / ("keep_lmv_%04d.png" % k))
         assert (w, h) == (80, 40)
+
+
+def _frame_fields_host(Q, g, h):
+    """fv_up7's frame fields from an FP32 padded primitive state, restated in
+    numpy (fv_up7_ducros_2d.cu:511-526, :800-829)."""
+    n = Q.shape[-1] - 2 * g
+    c = lambda q, dj, di: Q[q, g + dj:g + dj + n, g + di:g + di + n]
+    duc = lambda pa, pb: (pb - pa) ** 2 / ((pb - pa) ** 2 + np.float32(0.1) * (pb + pa) ** 2)
+    p = c(3, 0, 0)
+    sd = np.maximum(np.maximum(duc(p, c(3, 0, 1)), duc(c(3, 0, -1), p)),
+                    np.maximum(duc(p, c(3, 1, 0)), duc(c(3, -1, 0), p)))
+    w6 = [(-3, -1.0), (-2, 9.0), (-1, -45.0), (1, 45.0), (2, -9.0), (3, 1.0)]
+    dvdx = sum(np.float32(k) * c(2, 0, o) for o, k in w6)
+    dudy = sum(np.float32(k) * c(1, o, 0) for o, k in w6)
+    vort = (dvdx - dudy) / np.float32(60.0 * h)
+    speed = np.sqrt(c(1, 0, 0) ** 2 + c(2, 0, 0) ** 2)
+    return {"rho": c(0, 0, 0), "vorticity": vort, "ducros": sd, "speed": speed, "p": p}
+
+
+@pytest.mark.parametrize("case,bc,prec", [("sod", "reflect", "f64"), ("kh", "periodic", "f32c"),
+                                          ("vortex", "periodic", "f32")])
+def test_device_frame_fields_match_host_restatement(case, bc, prec):
+    n = 96
+    kw = dict(x0=-5, y0=-5, length=10.0) if case == "vortex" else {}
+    s = F.Solver(n, bc=bc, precision=prec, cfl=0.4, **kw)
+    s.init_case(case)
+    s.step(20)
+    Q = s.get_state(dtype=np.float32)   # the state the frame sees
+    s.frame_begin()
+    s.step(7)                           # overlaps the frame's copy
+    fr = s.frame_end()
+    ref = _frame_fields_host(Q, s.g, 10.0 / n if case == "vortex" else 1.0 / n)
+    for k in ("rho", "p", "speed", "ducros"):
+        assert np.allclose(fr[k], ref[k], rtol=2e-6, atol=1e-7), k
+    scale = max(float(np.abs(ref["vorticity"]).max()), 1e-6)
+    assert np.abs(fr["vorticity"] - ref["vorticity"]).max() <= 1e-5 * scale
+    assert s.sync().steps == 27
