@@ -15,7 +15,7 @@ LIB_PATH = Path(os.environ.get("FVB_LIBRARY", Path(__file__).resolve().parent / 
 
 # enums (include/fvb.h)
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_BLOWUP, ERR_DT_UNDERFLOW, ERR_NOT_FOUND, ERR_TIMEOUT = range(8)
-FLUX = {"up_ducros": 0, "keep": 1}
+FLUX = {"up_ducros": 0, "keep": 1, "up_ducros_hll": 2, "up_ducros_roe": 3}
 PREC = {"f64": 0, "f32": 1, "f32c": 2}
 BC = {"reflect": 0, "periodic": 1, "transmissive": 2}
 LAYOUT = {"prim": 0, "cons": 1}

@@ -143,6 +143,7 @@ struct fvb_solver {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int graph_steps = 1;
     bool keep = false;  // KEEP flux family: conserved FP64 state, g = 2
+    int rs = 0;         // solver on the reconstructed states: 0 HLLC, 1 HLL, 2 Roe
     // frame extraction (fvb_frame_begin / fvb_frame_end)
     float *frame_prim = nullptr;   // device, FP32 primitives with ghosts
     float *frame_dev = nullptr;    // device, 5 n x n fields
@@ -186,7 +187,7 @@ static cudaError_t enqueue_steps_direct(fvb_solver *s, int nsteps)
         }
         for (int stage = 1; stage <= 3; ++stage) {
             StageArgs a = stage_args(s, stage, s->parity);
-            cudaError_t e = launch_stage(s->prec, s->order, s->shape, a, s->ctas, s->stream);
+            cudaError_t e = launch_stage(s->prec, s->order, s->shape, a, s->ctas, s->stream, s->rs);
             if (e != cudaSuccess) return e;
         }
         if (s->prec == FVB_PREC_F32C) s->parity ^= 1;
@@ -293,7 +294,11 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     if (!cfg || !out) return fail(FVB_ERR_INVALID, "null argument");
     *out = nullptr;
     const bool keep = cfg->flux == FVB_FLUX_KEEP;
-    if (cfg->flux != FVB_FLUX_UP_DUCROS && !keep) return fail(FVB_ERR_INVALID, "unknown flux %d", cfg->flux);
+    const int rs = cfg->flux == FVB_FLUX_UP_DUCROS_HLL ? 1 : cfg->flux == FVB_FLUX_UP_DUCROS_ROE ? 2 : 0;
+    if (cfg->flux != FVB_FLUX_UP_DUCROS && !keep && rs == 0)
+        return fail(FVB_ERR_INVALID, "unknown flux %d", cfg->flux);
+    if (rs && !(cfg->precision == FVB_PREC_F64 && cfg->order == 7))
+        return fail(FVB_ERR_INVALID, "the HLL / Roe variants are built for FP64, order 7");
     if (cfg->precision < 0 || cfg->precision > 2) return fail(FVB_ERR_INVALID, "unknown precision %d", cfg->precision);
     if (keep && cfg->precision != FVB_PREC_F64)
         return fail(FVB_ERR_INVALID, "the KEEP flux family runs in FP64 (as keep_fv_euler_2d.cu)");
@@ -319,6 +324,7 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     s->g = g;
     s->n = cfg->n;
     s->keep = keep;
+    s->rs = rs;
     s->internal = keep ? INT_CONS64 : prec_internal(s->prec);
     s->G = make_geometry(cfg->n, g, s->prec);
     if (cfg->stream) s->stream = (cudaStream_t)cfg->stream;
@@ -372,7 +378,7 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
         }
     }
     {
-        int per_sm = stage_max_ctas_per_sm(s->prec, s->order, s->shape), sms = 0;
+        int per_sm = stage_max_ctas_per_sm(s->prec, s->order, s->shape, s->rs), sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device);
         s->ctas = std::min(s->tiles, std::max(1, per_sm) * std::max(1, sms));
     }
@@ -381,7 +387,7 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     e = ctrl_set(s->ctrl, 0.0, 1, 0.0, cfg->cfl, s->gd.h, s->stream);
     if (e != cudaSuccess) { fvb_destroy(s); return cuda_fail(e, "step control"); }
     // make sure the kernel variant can launch on this device
-    if (stage_max_ctas_per_sm(s->prec, s->order, s->shape) <= 0) {
+    if (stage_max_ctas_per_sm(s->prec, s->order, s->shape, s->rs) <= 0) {
         fvb_destroy(s);
         return fail(FVB_ERR_CUDA, "stage kernel variant cannot be resident on this device");
     }

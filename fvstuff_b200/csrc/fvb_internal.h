@@ -111,10 +111,11 @@ size_t stage32c_smem(int shape);
 // time / step advance in stage 3) and writes the TileCtl the stage reads.
 cudaError_t launch_stage_control(int prec, Ctrl *ctrl, int count, int stage, TileCtl *out, cudaStream_t s);
 
-// launchers (fvb_stage.cu)
+// launchers (fvb_stage.cu).  rs: the solver on the reconstructed states of
+// the FP64 UP7 kernel -- 0 HLLC, 1 HLL, 2 Roe
 cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int grid_ctas,
-                         cudaStream_t s);
-size_t stage_smem_bytes(int prec, int order, int shape);
-int stage_max_ctas_per_sm(int prec, int order, int shape);
+                         cudaStream_t s, int rs = 0);
+size_t stage_smem_bytes(int prec, int order, int shape, int rs = 0);
+int stage_max_ctas_per_sm(int prec, int order, int shape, int rs = 0);
 
 }  // namespace fvb

@@ -259,15 +259,91 @@ __device__ __forceinline__ void cell_ce(R r, R a, R b, R p, const GasF<R> &gs, R
 // s the pressure-jump sensor of the two cells.  L, Rv: floored UP
 // reconstructions; WL, WR: cell states with their sound speeds cW* and
 // energies EW*.                               fv_up7_ducros_2d.cu:237-328, :433
+//
+// RS selects the solver on the reconstructed states: 0 HLLC (fv_up7), 1 HLL,
+// 2 Roe with the Harten-Hyman entropy fix (carb_fv_2d.cu:116-211, the
+// riemann_n alternatives of carb_fv), always blended with the HLLE of the
+// cell states by the Ducros sensor.
 template <class R>
+__device__ __forceinline__ void hll_fast(const R L[4], const R Rv[4], const GasF<R> &gs, R Fh[4])
+{
+    const R zero = R(0);
+    const R rL = L[0], uL = L[1], tL = L[2], pL = L[3];
+    const R rR = Rv[0], uR = Rv[1], tR = Rv[2], pR = Rv[3];
+    const R ip = frcp(rL * rR);
+    // sound speed without a floor, as carb_fv_2d.cu:60-61 (rho, p >= 1e-14)
+    const R cL = fsqrt(gs.gam * pL * (rR * ip)), cR = fsqrt(gs.gam * pR * (rL * ip));
+    const R EL = pL * gs.igm1 + R(0.5) * rL * (uL * uL + tL * tL);
+    const R ER = pR * gs.igm1 + R(0.5) * rR * (uR * uR + tR * tR);
+    // Einfeldt's form of the two-wave average: FL, FR or the subsonic
+    // average without selects
+    const R SL = dmin<R>(dmin<R>(uL - cL, uR - cR), zero), SR = dmax<R>(dmax<R>(uL + cL, uR + cR), zero);
+    const R inv = frcp(SR - SL), SRL = SR * SL;
+    const R mL = rL * uL, mR = rR * uR;
+    Fh[0] = (SR * mL - SL * mR + SRL * (rR - rL)) * inv;
+    Fh[1] = (SR * (mL * uL + pL) - SL * (mR * uR + pR) + SRL * (mR - mL)) * inv;
+    Fh[2] = (SR * (mL * tL) - SL * (mR * tR) + SRL * (rR * tR - rL * tL)) * inv;
+    Fh[3] = (SR * ((EL + pL) * uL) - SL * ((ER + pR) * uR) + SRL * (ER - EL)) * inv;
+}
+
+template <class R>
+__device__ __forceinline__ void roe_fast(const R L[4], const R Rv[4], const GasF<R> &gs, R Fh[4])
+{
+    const R zero = R(0);
+    const R rL = L[0], uL = L[1], tL = L[2], pL = L[3];
+    const R rR = Rv[0], uR = Rv[1], tR = Rv[2], pR = Rv[3];
+    const R ip = frcp(rL * rR);
+    const R irL = rR * ip, irR = rL * ip;
+    const R cL = fsqrt(gs.gam * pL * irL), cR = fsqrt(gs.gam * pR * irR);
+    const R sqL = fsqrt(rL), sqR = fsqrt(rR);
+    const R iden = frcp(sqL + sqR);
+    const R a = (sqL * uL + sqR * uR) * iden, b = (sqL * tL + sqR * tR) * iden;  // Roe normal / tangential velocity
+    const R EL = pL * gs.igm1 + R(0.5) * rL * (uL * uL + tL * tL);
+    const R ER = pR * gs.igm1 + R(0.5) * rR * (uR * uR + tR * tR);
+    const R H = (sqL * ((EL + pL) * irL) + sqR * ((ER + pR) * irR)) * iden;
+    const R c2 = gs.gm1 * (H - R(0.5) * (a * a + b * b));
+    const R c = fsqrt(c2 > FVB_LIT(R, 1e-14) ? c2 : FVB_LIT(R, 1e-14));
+    const R ic2 = frcp(c2);
+    const R drho = rR - rL, dun = uR - uL, dut = tR - tL, dp = pR - pL;
+    const R rr = sqL * sqR;
+    const R b1 = (dp - rr * c * dun) * (R(0.5) * ic2);
+    const R b2 = drho - dp * ic2;
+    const R b3 = rr * dut;
+    const R b4 = (dp + rr * c * dun) * (R(0.5) * ic2);
+    // Harten-Hyman: |lambda| below eps/2 replaced by (lambda^2 + eps^2/4)/eps
+    const R lam1 = a - c, lam4 = a + c;
+    const R eps1 = dmax<R>(zero, R(2) * ((uR - cR) - (uL - cL)));
+    const R eps4 = dmax<R>(zero, R(2) * ((uR + cR) - (uL + cL)));
+    R al1 = dabs<R>(lam1), al4 = dabs<R>(lam4);
+    const R al2 = dabs<R>(a);
+    al1 = al1 < eps1 * R(0.5) ? (lam1 * lam1 + eps1 * eps1 * R(0.25)) * frcp(eps1) : al1;
+    al4 = al4 < eps4 * R(0.5) ? (lam4 * lam4 + eps4 * eps4 * R(0.25)) * frcp(eps4) : al4;
+    const R w1 = al1 * b1, w2 = al2 * b2, w3 = al2 * b3, w4 = al4 * b4;
+    const R d0 = w1 + w2 + w4;
+    const R d1 = w1 * lam1 + w2 * a + w4 * lam4;
+    const R d2 = (w1 + w2 + w4) * b + w3;
+    const R d3 = w1 * (H - a * c) + w2 * R(0.5) * (a * a + b * b) + w3 * b + w4 * (H + a * c);
+    const R mL = rL * uL, mR = rR * uR;
+    Fh[0] = R(0.5) * (mL + mR - d0);
+    Fh[1] = R(0.5) * (mL * uL + pL + mR * uR + pR - d1);
+    Fh[2] = R(0.5) * (mL * tL + mR * tR - d2);
+    Fh[3] = R(0.5) * ((EL + pL) * uL + (ER + pR) * uR - d3);
+}
+
+template <class R, int RS = 0>
 __device__ __forceinline__ void face_flux_fast(const R L[4], const R Rv[4], const R WL[4], const R WR[4], R cWL,
                                                R cWR, R EWL, R EWR, const GasF<R> &gs, R F[4])
 {
     const R zero = R(0);
-    // --- HLLC of the reconstructed states (branch-free, so the HLLC and HLLE
-    // chains share one basic block and interleave) ---
+    // --- solver on the reconstructed states (branch-free, so its chain and
+    // the HLLE chain share one basic block and interleave) ---
     R Fh0, Fh1, Fh2, Fh3;
-    {
+    if constexpr (RS == 1 || RS == 2) {
+        R Fh[4];
+        if constexpr (RS == 1) hll_fast<R>(L, Rv, gs, Fh);
+        else roe_fast<R>(L, Rv, gs, Fh);
+        Fh0 = Fh[0]; Fh1 = Fh[1]; Fh2 = Fh[2]; Fh3 = Fh[3];
+    } else {
         const R rL = L[0], uL = L[1], tL = L[2], pL = L[3];
         const R rR = Rv[0], uR = Rv[1], tR = Rv[2], pR = Rv[3];
         R irL, irR;

@@ -29,7 +29,7 @@ namespace fvb {
 // Flux through one face of the working tile W ([6][SH][SW]: rho, u, v, p,
 // c, E) whose right/top cell is at `base`; XDIR: x-face (normal u), else
 // y-face (normal v).  Writes the 4 Cartesian components to out[q * ostride].
-template <int PREC, int ORDER, int SW, int PL, bool XDIR, class R>
+template <int PREC, int ORDER, int SW, int PL, bool XDIR, int RS, class R>
 __device__ __forceinline__ void face_one(const R *W, int base, R *out, int ostride, const GasF<R> &gf,
                                          const Gas<R> &gs)
 {
@@ -55,7 +55,7 @@ __device__ __forceinline__ void face_one(const R *W, int base, R *out, int ostri
     R Fn[4];
     if constexpr (PREC != P32) {
         const R *CE = W + 4 * PL + base;
-        face_flux_fast<R>(L, Rv, WL, WR, CE[-ST], CE[0], CE[PL - ST], CE[PL], gf, Fn);
+        face_flux_fast<R, RS>(L, Rv, WL, WR, CE[-ST], CE[0], CE[PL - ST], CE[PL], gf, Fn);
     } else {
         R Fh[4], Fl[4];
         hllc<R>(L, Rv, Fh, gs);
@@ -73,7 +73,7 @@ __device__ __forceinline__ void face_one(const R *W, int base, R *out, int ostri
 
 // The FP64 and FP32 (reference-rounding) stage kernel, two CTAs per SM; the
 // FP32-compensated form has its own kernel (fvb_stage32c.cu).
-template <int PREC, int ORDER, int TX, int TY, int NT, bool BATCHED, int MINB>
+template <int PREC, int ORDER, int TX, int TY, int NT, bool BATCHED, int MINB, int RS>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__ StageArgs a)
 {
     static_assert(PREC == P64 || PREC == P32, "FP64 and FP32 primitive-state forms");
@@ -233,12 +233,12 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         // ---- 3. face fluxes: x-faces, then y-faces (compile-time strides) ---
         for (int f = tid; f < NXF; f += NT) {
             const int r = f / (TX + 1), c = f - r * (TX + 1);
-            face_one<PREC, ORDER, SW, PL, true>(W, (r + G) * SW + (c + G), FX + r * (TX + 1) + c, TY * (TX + 1),
+            face_one<PREC, ORDER, SW, PL, true, RS>(W, (r + G) * SW + (c + G), FX + r * (TX + 1) + c, TY * (TX + 1),
                                                gf, gs);
         }
         for (int f = tid; f < NYF; f += NT) {
             const int r = f / TX, c = f - r * TX;
-            face_one<PREC, ORDER, SW, PL, false>(W, (r + G) * SW + (c + G), FY + r * TX + c, (TY + 1) * TX, gf,
+            face_one<PREC, ORDER, SW, PL, false, RS>(W, (r + G) * SW + (c + G), FY + r * TX + c, (TY + 1) * TX, gf,
                                                 gs);
         }
         __syncthreads();
@@ -393,7 +393,7 @@ cudaError_t launch_stage_control(int prec, Ctrl *ctrl, int count, int stage, Til
 // ---------------------------------------------------------------------------
 // instantiation table
 // ---------------------------------------------------------------------------
-template <int PREC, int ORDER, int SHAPE>
+template <int PREC, int ORDER, int SHAPE, int RS = 0>
 struct K {
     static constexpr TileShape ts = kTileShapes[SHAPE];
     static constexpr int G = (ORDER + 1) / 2;
@@ -404,8 +404,8 @@ struct K {
     // shared memory fits in the SM's 228 KB (1 KB reserved per CTA), else two
     static constexpr int kMinBlocks = 3 * (kSmem + 1024) <= 228 * 1024 ? 3 : 2;
     static size_t smem() { return kSmem; }
-    static void *fn() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt, false, kMinBlocks>; }
-    static void *fn_batched() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt, true, kMinBlocks>; }
+    static void *fn() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt, false, kMinBlocks, RS>; }
+    static void *fn_batched() { return (void *)stage_kernel<PREC, ORDER, ts.tx, ts.ty, ts.nt, true, kMinBlocks, RS>; }
 };
 
 struct KernelEntry {
@@ -417,11 +417,11 @@ struct KernelEntry {
     int max_ctas;
 };
 
-template <int PREC, int ORDER, int SHAPE>
+template <int PREC, int ORDER, int SHAPE, int RS = 0>
 static KernelEntry entry()
 {
-    return KernelEntry{K<PREC, ORDER, SHAPE>::fn(), K<PREC, ORDER, SHAPE>::fn_batched(),
-                       K<PREC, ORDER, SHAPE>::smem(), kTileShapes[SHAPE].nt, 0, 0};
+    using KK = K<PREC, ORDER, SHAPE, RS>;
+    return KernelEntry{KK::fn(), KK::fn_batched(), KK::smem(), kTileShapes[SHAPE].nt, 0, 0};
 }
 
 static KernelEntry entry32c(int shape)
@@ -432,9 +432,15 @@ static KernelEntry entry32c(int shape)
 
 #define FVB_SHAPES(P, O) \
     entry<P, O, 0>(), entry<P, O, 1>(), entry<P, O, 2>(), entry<P, O, 3>(), entry<P, O, 4>(), entry<P, O, 5>()
+#define FVB_SHAPES_RS(RS) \
+    entry<P64, 7, 0, RS>(), entry<P64, 7, 1, RS>(), entry<P64, 7, 2, RS>(), entry<P64, 7, 3, RS>(), \
+        entry<P64, 7, 4, RS>(), entry<P64, 7, 5, RS>()
 
-static KernelEntry *table_for(int prec, int order)
+static KernelEntry *table_for(int prec, int order, int rs = 0)
 {
+    static KernelEntry t64_7_hll[] = {FVB_SHAPES_RS(1)};
+    static KernelEntry t64_7_roe[] = {FVB_SHAPES_RS(2)};
+    if (rs != 0) return (prec == P64 && order == 7) ? (rs == 1 ? t64_7_hll : rs == 2 ? t64_7_roe : nullptr) : nullptr;
     static KernelEntry t64_7[] = {FVB_SHAPES(P64, 7)};
     static KernelEntry t64_5[] = {FVB_SHAPES(P64, 5)};
     static KernelEntry t64_3[] = {FVB_SHAPES(P64, 3)};
@@ -535,23 +541,23 @@ cudaError_t put_tile_maps(const CUtensorMap maps[TM_COUNT], CUtensorMap *dst, cu
     return cudaGetLastError();
 }
 
-size_t stage_smem_bytes(int prec, int order, int shape)
+size_t stage_smem_bytes(int prec, int order, int shape, int rs)
 {
-    KernelEntry *t = table_for(prec, order);
+    KernelEntry *t = table_for(prec, order, rs);
     return t ? t[shape].smem : 0;
 }
 
-int stage_max_ctas_per_sm(int prec, int order, int shape)
+int stage_max_ctas_per_sm(int prec, int order, int shape, int rs)
 {
-    KernelEntry *t = table_for(prec, order);
+    KernelEntry *t = table_for(prec, order, rs);
     if (!t || shape < 0 || shape >= kNumTileShapes) return 0;
     if (prepare(t[shape]) != cudaSuccess) return 0;
     return t[shape].max_ctas;
 }
 
-cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int grid_ctas, cudaStream_t s)
+cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int grid_ctas, cudaStream_t s, int rs)
 {
-    KernelEntry *t = table_for(prec, order);
+    KernelEntry *t = table_for(prec, order, rs);
     if (!t || shape < 0 || shape >= kNumTileShapes) return cudaErrorInvalidValue;
     KernelEntry &e = t[shape];
     cudaError_t err = prepare(e);

@@ -44,7 +44,11 @@ typedef enum fvb_status {
 
 typedef enum fvb_flux {
     FVB_FLUX_UP_DUCROS = 0,   /* UP-order recon + Ducros HLLC/HLLE (fv_up7_ducros_2d.cu:370-507) */
-    FVB_FLUX_KEEP = 1         /* ECKEP + JST/MOVERS-RH (keep_fv_euler_2d.cu:298-369)              */
+    FVB_FLUX_KEEP = 1,        /* ECKEP + JST/MOVERS-RH (keep_fv_euler_2d.cu:298-369)              */
+    /* UP7 + Ducros blend with carb_fv's alternatives to HLLC on the
+     * reconstructed states (carb_fv_2d.cu:116-211; FP64, order 7) */
+    FVB_FLUX_UP_DUCROS_HLL = 2,
+    FVB_FLUX_UP_DUCROS_ROE = 3
 } fvb_flux;
 
 typedef enum fvb_precision {

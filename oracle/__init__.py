@@ -82,15 +82,20 @@ def padded(N: int, g: int, dtype=np.float64) -> np.ndarray:
 # ---------------------------------------------------------------------------
 # restatement (liboracle.so)
 # ---------------------------------------------------------------------------
-def up_rhs(Q: np.ndarray, N: int, h: float, order: int = 7):
-    """Residual (4,N,N) and lam (N,N) of a padded primitive state."""
+RIEMANN = {"hllc": 0, "hll": 1, "roe": 2}
+
+
+def up_rhs(Q: np.ndarray, N: int, h: float, order: int = 7, riemann: str = "hllc"):
+    """Residual (4,N,N) and lam (N,N) of a padded primitive state; `riemann`
+    picks the solver on the reconstructed states (fv_up7's HLLC, or carb_fv's
+    HLL / Roe)."""
     g = ghost_width(order)
     assert Q.shape == (4, N + 2 * g, N + 2 * g) and Q.flags.c_contiguous
     s = _sfx(Q.dtype)
     R = np.empty((4, N, N), Q.dtype)
     lam = np.empty((N, N), Q.dtype)
     getattr(lib(), "orc_up_rhs_" + s)(_ptr(Q), _ptr(R), _ptr(lam), C.c_int(N), C.c_int(g),
-                                      C.c_int(order), _real(Q.dtype)(h))
+                                      C.c_int(order + 100 * RIEMANN[riemann]), _real(Q.dtype)(h))
     return R, lam
 
 
@@ -104,13 +109,14 @@ def rk3(stage, Uo, U0, Uk, L, dt, N, g) -> None:
 
 
 def up_run(U: np.ndarray, N: int, h: float, cfl: float, bc_kind: int, max_steps: int,
-           t_stop: float = 1e30, order: int = 7):
+           t_stop: float = 1e30, order: int = 7, riemann: str = "hllc"):
     """Advance U (padded primitives, ghosts filled) in place; returns
     (status, t, steps, lam_max, last_dt)."""
     g = ghost_width(order)
     info = np.zeros(4)
     st = getattr(lib(), "orc_up_run_" + _sfx(U.dtype))(
-        _ptr(U), C.c_int(N), C.c_int(g), C.c_int(order), C.c_int(bc_kind), _real(U.dtype)(h),
+        _ptr(U), C.c_int(N), C.c_int(g), C.c_int(order + 100 * RIEMANN[riemann]), C.c_int(bc_kind),
+        _real(U.dtype)(h),
         _real(U.dtype)(cfl), C.c_int(max_steps), C.c_double(t_stop), _ptr(info))
     return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3])
 
@@ -125,6 +131,34 @@ def ic_sod(N: int, h: float, dtype=np.float64, order: int = 7) -> np.ndarray:
 def hllc(L, R, dtype=np.float64):
     L = np.ascontiguousarray(L, dtype); R = np.ascontiguousarray(R, dtype); F = np.empty(4, dtype)
     getattr(lib(), "orc_hllc_" + _sfx(dtype))(_ptr(L), _ptr(R), _ptr(F))
+    return F
+
+
+def hll(L, R):
+    """carb_fv's HLL flux, FP64, normal frame."""
+    L, R = np.ascontiguousarray(L, np.float64), np.ascontiguousarray(R, np.float64)
+    F = np.empty(4)
+    lib().orc_hll_f64(_ptr(L), _ptr(R), _ptr(F))
+    return F
+
+
+def roe(L, R):
+    """carb_fv's Roe flux with the Harten-Hyman fix, FP64, normal frame."""
+    L, R = np.ascontiguousarray(L, np.float64), np.ascontiguousarray(R, np.float64)
+    F = np.empty(4)
+    lib().orc_roe_f64(_ptr(L), _ptr(R), _ptr(F))
+    return F
+
+
+def have_ref_carb() -> bool:
+    return (REF / "libref_host_carb.so").exists()
+
+
+def ref_carb_flux(kind: str, WL, WR, nx: float, ny: float):
+    """carb_fv_2d.cu's own hll_n / roe_n / hllc_n, compiled for the host."""
+    WL, WR = np.ascontiguousarray(WL, np.float64), np.ascontiguousarray(WR, np.float64)
+    F = np.empty(4)
+    getattr(ref_host("carb"), "ref_carb_" + kind)(_ptr(WL), _ptr(WR), C.c_double(nx), C.c_double(ny), _ptr(F))
     return F
 
 

@@ -40,6 +40,9 @@ KEEP = "keep_fv_euler_2d.cu"
 # its <<<>>> launches, image output and main.
 UP7_HOST_LINES = [(26, 38), (48, 590), (614, 639)]
 KEEP_HOST_LINES = [(46, 68), (78, 393), (441, 536)]
+CARB = "carb_fv_2d.cu"
+# GAMMA_V and the `real` switch, then sound_speed, hllc_n, hll_n and roe_n
+CARB_HOST_LINES = [(36, 36), (40, 44), (60, 211)]
 
 NVCC = os.environ.get("NVCC", "nvcc")
 GPU_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -107,6 +110,9 @@ def build_ref(verbose: bool = False, gpu: bool = True) -> list[Path]:
     _write_if_changed(OUT / "up7_host_f32.inc", _extract(up7, UP7_HOST_LINES))
     _write_if_changed(OUT / "up7_host_f64.inc", retype_f64(_extract(up7, UP7_HOST_LINES)))
     _write_if_changed(OUT / "keep_host.inc", _extract(keep, KEEP_HOST_LINES))
+    carb = REF_DIR / CARB
+    if carb.exists():
+        _write_if_changed(OUT / "carb_host.inc", _extract(carb, CARB_HOST_LINES))
     _write_if_changed(OUT / "fv_up7_f64.cu", retype_f64(up7_text))
 
     host_flags = ["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared",
@@ -118,6 +124,9 @@ def build_ref(verbose: bool = False, gpu: bool = True) -> list[Path]:
                                     '-DREF_INC="_ref/up7_host_f64.inc"'], OUT / "up7_host_f64.inc"),
         ("libref_host_keep.so", ["-DREF_KEEP", '-DREF_INC="_ref/keep_host.inc"'], OUT / "keep_host.inc"),
     ]
+    if carb.exists():
+        host.append(("libref_host_carb.so", ["-DREF_CARB", "-DUSE_DOUBLE", '-DREF_INC="_ref/carb_host.inc"'],
+                     OUT / "carb_host.inc"))
     built = []
     for name, defs, inc in host:
         out = OUT / name

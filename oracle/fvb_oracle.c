@@ -52,5 +52,7 @@ void orc_hllc_f64(const double L[4], const double R[4], double F[4]) { hllc_f64(
 void orc_hlle_f64(const double L[4], const double R[4], double F[4]) { hlle_f64(L, R, F); }
 void orc_hllc_f32(const float L[4], const float R[4], float F[4]) { hllc_f32(L, R, F); }
 void orc_hlle_f32(const float L[4], const float R[4], float F[4]) { hlle_f32(L, R, F); }
+void orc_hll_f64(const double L[4], const double R[4], double F[4]) { hll_f64(L, R, F); }
+void orc_roe_f64(const double L[4], const double R[4], double F[4]) { roe_f64(L, R, F); }
 void orc_upface_f64(int order, const double *s, double *vL, double *vR) { upface_f64(order, s, vL, vR); }
 void orc_upface_f32(int order, const float *s, float *vL, float *vR) { upface_f32(order, s, vL, vR); }

@@ -162,13 +162,83 @@ static void OSFX(hlle)(const REAL L[4], const REAL R[4], REAL F[4])
         F[q] = (SR * FL[q] - SL * FR[q] + SR * SL * (UR[q] - UL[q])) / dS;
 }
 
+/* ---- Riemann-solver variants of carb_fv_2d.cu, normal frame ------------
+ * (The reference's rotation by n = (1,0) or (0,1) reduces to the same
+ * relabelling as above; for (0,1) its tangential velocity is -u, which only
+ * flips the sign of the tangential terms and is undone by its back-rotation,
+ * exactly, since negation is exact.)  Sound speed as carb_fv_2d.cu:60-61,
+ * without the 1e-14 floor of fv_up7.                                        */
+static inline REAL OSFX(snd_carb)(REAL rho, REAL p) { return OSQRT(RL(1.4) * p / rho); }
+
+/* HLL, two waves with Davis bounds             carb_fv_2d.cu:116-150 */
+static void OSFX(hll)(const REAL L[4], const REAL R[4], REAL F[4])
+{
+    REAL rL = L[0], uL = L[1], tL = L[2], pL = L[3];
+    REAL rR = R[0], uR = R[1], tR = R[2], pR = R[3];
+    REAL cL = OSFX(snd_carb)(rL, pL), cR = OSFX(snd_carb)(rR, pR);
+    REAL EL = OSFX(etot)(rL, uL, tL, pL), ER = OSFX(etot)(rR, uR, tR, pR);
+    REAL SL = OFMIN(uL - cL, uR - cR);
+    REAL SR = OFMAX(uL + cL, uR + cR);
+    REAL FL[4] = { rL * uL, rL * uL * uL + pL, rL * uL * tL, (EL + pL) * uL };
+    REAL FR[4] = { rR * uR, rR * uR * uR + pR, rR * uR * tR, (ER + pR) * uR };
+    if (SL >= RL(0.)) { for (int q = 0; q < 4; q++) F[q] = FL[q]; return; }
+    if (SR <= RL(0.)) { for (int q = 0; q < 4; q++) F[q] = FR[q]; return; }
+    REAL UL[4] = { rL, rL * uL, rL * tL, EL };
+    REAL UR[4] = { rR, rR * uR, rR * tR, ER };
+    REAL inv = RL(1.) / (SR - SL);
+    for (int q = 0; q < 4; q++) F[q] = (SR * FL[q] - SL * FR[q] + SL * SR * (UR[q] - UL[q])) * inv;
+}
+
+/* Roe with the Harten-Hyman entropy fix        carb_fv_2d.cu:153-211 */
+static void OSFX(roe)(const REAL L[4], const REAL R[4], REAL F[4])
+{
+    REAL rL = L[0], uL = L[1], tL = L[2], pL = L[3];
+    REAL rR = R[0], uR = R[1], tR = R[2], pR = R[3];
+    REAL cL = OSFX(snd_carb)(rL, pL), cR = OSFX(snd_carb)(rR, pR);
+    REAL sqL = OSQRT(rL), sqR = OSQRT(rR);
+    REAL den = sqL + sqR;
+    REAL aRoe = (sqL * uL + sqR * uR) / den;   /* normal velocity      */
+    REAL bRoe = (sqL * tL + sqR * tR) / den;   /* tangential velocity  */
+    REAL HL = (pL / (RL(1.4) - RL(1.)) + RL(0.5) * rL * (uL * uL + tL * tL) + pL) / rL;
+    REAL HR = (pR / (RL(1.4) - RL(1.)) + RL(0.5) * rR * (uR * uR + tR * tR) + pR) / rR;
+    REAL HRoe = (sqL * HL + sqR * HR) / den;
+    REAL c2 = (RL(1.4) - RL(1.)) * (HRoe - RL(0.5) * (aRoe * aRoe + bRoe * bRoe));
+    REAL cRoe = OSQRT(c2 > RL(1e-14) ? c2 : RL(1e-14));
+    REAL EL = OSFX(etot)(rL, uL, tL, pL), ER = OSFX(etot)(rR, uR, tR, pR);
+    REAL FL[4] = { rL * uL, rL * uL * uL + pL, rL * uL * tL, (EL + pL) * uL };
+    REAL FR[4] = { rR * uR, rR * uR * uR + pR, rR * uR * tR, (ER + pR) * uR };
+    REAL drho = rR - rL, dun = uR - uL, dut = tR - tL, dp = pR - pL;
+    REAL rRoe = sqL * sqR;
+    REAL b1 = (dp - rRoe * cRoe * dun) / (RL(2.) * c2);
+    REAL b2 = drho - dp / c2;
+    REAL b3 = rRoe * dut;
+    REAL b4 = (dp + rRoe * cRoe * dun) / (RL(2.) * c2);
+    REAL lam1 = aRoe - cRoe, lam2 = aRoe, lam3 = aRoe, lam4 = aRoe + cRoe;
+    REAL eps1 = OFMAX(RL(0.), RL(2.) * ((uR - cR) - (uL - cL)));
+    REAL eps4 = OFMAX(RL(0.), RL(2.) * ((uR + cR) - (uL + cL)));
+    REAL al1 = OFABS(lam1);
+    if (al1 < eps1 * RL(0.5)) al1 = (lam1 * lam1 + eps1 * eps1 * RL(0.25)) / eps1;
+    REAL al2 = OFABS(lam2), al3 = OFABS(lam3);
+    REAL al4 = OFABS(lam4);
+    if (al4 < eps4 * RL(0.5)) al4 = (lam4 * lam4 + eps4 * eps4 * RL(0.25)) / eps4;
+    REAL d0 = al1 * b1 + al2 * b2 + al4 * b4;
+    REAL d1 = al1 * b1 * (aRoe - cRoe) + al2 * b2 * aRoe + al4 * b4 * (aRoe + cRoe);
+    REAL d2 = al1 * b1 * bRoe + al2 * b2 * bRoe + al3 * b3 + al4 * b4 * bRoe;
+    REAL d3 = al1 * b1 * (HRoe - aRoe * cRoe) + al2 * b2 * RL(0.5) * (aRoe * aRoe + bRoe * bRoe)
+            + al3 * b3 * bRoe + al4 * b4 * (HRoe + aRoe * cRoe);
+    F[0] = RL(0.5) * (FL[0] + FR[0]) - RL(0.5) * d0;
+    F[1] = RL(0.5) * (FL[1] + FR[1]) - RL(0.5) * d1;
+    F[2] = RL(0.5) * (FL[2] + FR[2]) - RL(0.5) * d2;
+    F[3] = RL(0.5) * (FL[3] + FR[3]) - RL(0.5) * d3;
+}
+
 /* Blended face flux between the cells at offsets -1 and 0 of a stencil
  * gathered along the normal (stride st from base index b):
  *   F = (1-s) HLLC(UP recon) + s HLLE(cell averages)
  * comp[] maps (rho,u,v,p) slots to the normal frame: {0,1,2,3} for x-faces,
  * {0,2,1,3} for y-faces.                       fv_up7_ducros_2d.cu:414-494 */
 static void OSFX(face)(const REAL *Q, size_t Np2, ptrdiff_t b, ptrdiff_t st,
-                       int order, const int comp[4], REAL F[4])
+                       int order, int rs, const int comp[4], REAL F[4])
 {
     int g = (order + 1) / 2;
     REAL s[10], L[4], R[4], WL[4], WR[4], Fh[4], Fl[4];
@@ -183,7 +253,11 @@ static void OSFX(face)(const REAL *Q, size_t Np2, ptrdiff_t b, ptrdiff_t st,
     R[0] = R[0] > RL(1e-14) ? R[0] : RL(1e-14);
     L[3] = L[3] > RL(1e-14) ? L[3] : RL(1e-14);
     R[3] = R[3] > RL(1e-14) ? R[3] : RL(1e-14);
-    OSFX(hllc)(L, R, Fh);
+    /* rs: the solver on the reconstructed states -- 0 HLLC (fv_up7), 1 HLL,
+     * 2 Roe (carb_fv_2d.cu's riemann_n choices) */
+    if (rs == 1) OSFX(hll)(L, R, Fh);
+    else if (rs == 2) OSFX(roe)(L, R, Fh);
+    else OSFX(hllc)(L, R, Fh);
     OSFX(hlle)(WL, WR, Fl);
     REAL sd = OSFX(ducros)(WL[3], WR[3]);
     REAL Fn[4];
@@ -202,6 +276,10 @@ void OSFX(orc_up_rhs)(const REAL *Q, REAL *RHS, REAL *lam, int N, int g,
                       int order, REAL h)
 {
     static const int cx[4] = { 0, 1, 2, 3 }, cy[4] = { 0, 2, 1, 3 };
+    /* order + 100 rs selects the solver on the reconstructed states:
+     * rs 0 HLLC (fv_up7), 1 HLL, 2 Roe (carb_fv_2d.cu:116-211) */
+    const int rs = order / 100;
+    order %= 100;
     int Np = N + 2 * g;
     size_t Np2 = (size_t)Np * Np, N2 = (size_t)N * N;
     REAL *Fx = (REAL *)malloc(sizeof(REAL) * 4 * (size_t)(N + 1) * N);
@@ -210,14 +288,14 @@ void OSFX(orc_up_rhs)(const REAL *Q, REAL *RHS, REAL *lam, int N, int g,
         for (int i = 0; i <= N; i++) {       /* x-face i-1/2 of row j */
             ptrdiff_t b = (ptrdiff_t)(j + g) * Np + (i + g);
             REAL F[4];
-            OSFX(face)(Q, Np2, b, 1, order, cx, F);
+            OSFX(face)(Q, Np2, b, 1, order, rs, cx, F);
             for (int q = 0; q < 4; q++) Fx[((size_t)q * N + j) * (N + 1) + i] = F[q];
         }
     for (int j = 0; j <= N; j++)             /* y-face j-1/2 of column i */
         for (int i = 0; i < N; i++) {
             ptrdiff_t b = (ptrdiff_t)(j + g) * Np + (i + g);
             REAL F[4];
-            OSFX(face)(Q, Np2, b, Np, order, cy, F);
+            OSFX(face)(Q, Np2, b, Np, order, rs, cy, F);
             for (int q = 0; q < 4; q++) Fy[((size_t)q * (N + 1) + j) * N + i] = F[q];
         }
     for (int j = 0; j < N; j++)

@@ -9,6 +9,7 @@
  *   -DREF_UP7 -DREF_REAL=float   fv_up7_ducros_2d.cu as shipped
  *   -DREF_UP7 -DREF_REAL=double  its float->double retype
  *   -DREF_KEEP                   keep_fv_euler_2d.cu (FP64 already)
+ *   -DREF_CARB -DUSE_DOUBLE      carb_fv_2d.cu's Riemann solvers, FP64
  * Used to pin the oracle restatement bit-for-bit and as the CPU baseline
  * ("kind": "reference") of bench.py.
  */
@@ -160,6 +161,15 @@ int API(ref_up7_run_)(R *U, int N, R h, R cfl, int bc, int max_steps, double t_s
     return status;
 }
 
+}  /* extern "C" */
+
+#elif defined(REF_CARB)
+/* carb_fv_2d.cu's Riemann solvers (real = double with -DUSE_DOUBLE) */
+
+extern "C" {
+void ref_carb_hllc(const real *WL, const real *WR, real nx, real ny, real *F) { hllc_n(WL, WR, nx, ny, F); }
+void ref_carb_hll(const real *WL, const real *WR, real nx, real ny, real *F) { hll_n(WL, WR, nx, ny, F); }
+void ref_carb_roe(const real *WL, const real *WR, real nx, real ny, real *F) { roe_n(WL, WR, nx, ny, F); }
 }  /* extern "C" */
 
 #elif defined(REF_KEEP)

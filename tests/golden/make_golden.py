@@ -6,7 +6,8 @@ fixtures are outputs of its kernels (fv_up7_ducros_2d.cu as shipped and
 retyped to FP64, keep_fv_euler_2d.cu) on small seeded inputs, frozen so the
 oracle restatement stays pinned where the reference checkout is absent.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every fixture
+    python tests/golden/make_golden.py carb     # carb_fv's HLL / Roe faces only
 """
 from __future__ import annotations
 
@@ -58,9 +59,29 @@ def _faces(dtype, seed=7, count=64):
     return out
 
 
+def _faces_carb(seed=11, count=64):
+    """random face states through carb_fv_2d.cu's own hll_n and roe_n (FP64),
+    x and y normals"""
+    rng = np.random.default_rng(seed)
+    WL = np.empty((count, 4)); WR = np.empty((count, 4))
+    WL[:, 0] = rng.uniform(0.1, 3, count); WR[:, 0] = rng.uniform(0.1, 3, count)
+    WL[:, 3] = rng.uniform(0.1, 5, count); WR[:, 3] = rng.uniform(0.1, 5, count)
+    WL[:, 1:3] = rng.uniform(-3, 3, (count, 2)); WR[:, 1:3] = rng.uniform(-3, 3, (count, 2))
+    out = {"WL": WL, "WR": WR}
+    for name in ("hll", "roe"):
+        for tag, (nx, ny) in (("x", (1.0, 0.0)), ("y", (0.0, 1.0))):
+            out["%s_%s" % (name, tag)] = np.array([O.ref_carb_flux(name, WL[k], WR[k], nx, ny)
+                                                   for k in range(count)])
+    return out
+
+
 def main() -> None:
     if not O.have_ref_host():
         raise SystemExit("oracle/_ref is not built (python oracle/build.py)")
+    if O.have_ref_carb():
+        np.savez_compressed(HERE / "faces_carb_f64.npz", **_faces_carb())
+    if sys.argv[1:] == ["carb"]:
+        return
     O.ref_set_threads(1)
     N = 16
     for dtype, sfx in ((np.float64, "f64"), (np.float32, "f32")):
