@@ -162,6 +162,96 @@ def ref_carb_flux(kind: str, WL, WR, nx: float, ny: float):
     return F
 
 
+# ---- fv_rec3_2d.cu (FP64, periodic, g = 2, N even) --------------------------
+REC3_CASES = {"sod": 0, "pv": 1, "lmv": 2}
+
+
+def rec3_p0(eps: float = 0.1) -> float:
+    """Gresho background pressure 1/(gamma eps^2) - 1/2 (fv_rec3_2d.cu:518)."""
+    return 1.0 / (1.4 * eps * eps) - 0.5
+
+
+def rec3_ic(N: int, h: float, case: str = "sod", p0: float = 0.0) -> np.ndarray:
+    U = np.zeros((4, N + 4, N + 4))
+    lib().orc_rec3_ic(_ptr(U), C.c_int(N), C.c_double(h), C.c_int(REC3_CASES[case]), C.c_double(p0))
+    return U
+
+
+def rec3_limit(U: np.ndarray, N: int) -> int:
+    return int(lib().orc_rec3_limit(_ptr(U), C.c_int(N)))
+
+
+def rec3_rhs(U: np.ndarray, N: int, h: float):
+    R = np.empty((4, N, N)); lam = np.empty((N, N))
+    lib().orc_rec3_rhs(_ptr(U), _ptr(R), _ptr(lam), C.c_int(N), C.c_double(h))
+    return R, lam
+
+
+def rec3_run(U: np.ndarray, N: int, h: float, cfl: float, max_steps: int, t_stop: float = 1e30):
+    """(status, t, steps, lam_max, last dt, brutal fixes); U advanced in place."""
+    info = np.zeros(5)
+    st = lib().orc_rec3_run(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(cfl), C.c_int(max_steps),
+                            C.c_double(t_stop), _ptr(info))
+    return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3]), int(info[4])
+
+
+def rec3_err(U: np.ndarray, N: int, h: float, case: str, p0: float = 0.0):
+    out = np.zeros(2)
+    lib().orc_rec3_err(_ptr(U), C.c_int(N), C.c_double(h), C.c_int(REC3_CASES[case]), C.c_double(p0), _ptr(out))
+    return float(out[0]), float(out[1])
+
+
+def rec3_hllc(L, R):
+    L, R = np.ascontiguousarray(L, np.float64), np.ascontiguousarray(R, np.float64)
+    F = np.empty(4)
+    lib().orc_rec3_hllc(_ptr(L), _ptr(R), _ptr(F))
+    return F
+
+
+def rec3_scale(Ub, U):
+    Ub, U = np.ascontiguousarray(Ub, np.float64), np.array(U, np.float64)
+    lib().orc_rec3_scale(_ptr(Ub), _ptr(U))
+    return U
+
+
+def have_ref_rec3() -> bool:
+    return (REF / "libref_host_rec3.so").exists()
+
+
+def ref_rec3(name: str):
+    f = getattr(ref_host("rec3"), "ref_rec3_" + name)
+    if name in ("limit", "run"):
+        f.restype = C.c_int
+    return f
+
+
+def ref_rec3_ic(N, h, case="sod", p0=0.0):
+    U = np.zeros((4, N + 4, N + 4))
+    ref_rec3("ic")(_ptr(U), C.c_int(N), C.c_int(N + 4), C.c_double(h), C.c_int(REC3_CASES[case]), C.c_double(p0))
+    return U
+
+
+def ref_rec3_rhs(U, N, h):
+    R = np.empty((4, N, N)); lam = np.empty((N, N))
+    ref_rec3("rhs")(_ptr(U), _ptr(R), _ptr(lam), C.c_int(N), C.c_int(N + 4), C.c_double(h))
+    return R, lam
+
+
+def ref_rec3_limit(U, N):
+    return int(ref_rec3("limit")(_ptr(U), C.c_int(N), C.c_int(N + 4)))
+
+
+def ref_rec3_bc(U, N):
+    ref_rec3("bc")(_ptr(U), C.c_int(N), C.c_int(N + 4))
+
+
+def ref_rec3_run(U, N, h, cfl, max_steps, t_stop=1e30):
+    info = np.zeros(5)
+    st = ref_rec3("run")(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(cfl), C.c_int(max_steps),
+                         C.c_double(t_stop), _ptr(info))
+    return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3]), int(info[4])
+
+
 def hlle(L, R, dtype=np.float64):
     L = np.ascontiguousarray(L, dtype); R = np.ascontiguousarray(R, dtype); F = np.empty(4, dtype)
     getattr(lib(), "orc_hlle_" + _sfx(dtype))(_ptr(L), _ptr(R), _ptr(F))
@@ -210,7 +300,7 @@ def keep_err_lmv(U: np.ndarray, N: int, h: float, eps: float = 0.1):
 # the reference's own kernels, host build (oracle/_ref/libref_host_*.so)
 # ---------------------------------------------------------------------------
 def ref_set_threads(n: int) -> None:
-    for k in ("up7_f32", "up7_f64", "keep"):
+    for k in ("up7_f32", "up7_f64", "keep", "carb", "rec3"):
         try:
             ref_host(k).ref_set_threads(C.c_int(n))
         except FileNotFoundError:

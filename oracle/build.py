@@ -43,6 +43,10 @@ KEEP_HOST_LINES = [(46, 68), (78, 393), (441, 536)]
 CARB = "carb_fv_2d.cu"
 # GAMMA_V and the `real` switch, then sound_speed, hllc_n, hll_n and roe_n
 CARB_HOST_LINES = [(36, 36), (40, 44), (60, 211)]
+REC3 = "fv_rec3_2d.cu"
+# constants and floors, then everything from IDX_P to the error kernel;
+# left out: includes, the CK() macro, the reductions, host code and main
+REC3_HOST_LINES = [(36, 60), (65, 447)]
 
 NVCC = os.environ.get("NVCC", "nvcc")
 GPU_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -91,7 +95,8 @@ def _write_if_changed(p: Path, text: str) -> None:
 
 def build_oracle(verbose: bool = False) -> Path:
     out = HERE / "liboracle.so"
-    deps = [HERE / "fvb_oracle.c", HERE / "fvb_oracle_up7.h", HERE / "fvb_oracle_keep.h", HERE / "build.py"]
+    deps = [HERE / "fvb_oracle.c", HERE / "fvb_oracle_up7.h", HERE / "fvb_oracle_keep.h",
+            HERE / "fvb_oracle_rec3.h", HERE / "build.py"]
     if _stale(out, deps):
         _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off",
               "-o", str(out), str(HERE / "fvb_oracle.c"), "-lm"])
@@ -113,6 +118,9 @@ def build_ref(verbose: bool = False, gpu: bool = True) -> list[Path]:
     carb = REF_DIR / CARB
     if carb.exists():
         _write_if_changed(OUT / "carb_host.inc", _extract(carb, CARB_HOST_LINES))
+    rec3 = REF_DIR / REC3
+    if rec3.exists():
+        _write_if_changed(OUT / "rec3_host.inc", _extract(rec3, REC3_HOST_LINES))
     _write_if_changed(OUT / "fv_up7_f64.cu", retype_f64(up7_text))
 
     host_flags = ["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared",
@@ -127,6 +135,9 @@ def build_ref(verbose: bool = False, gpu: bool = True) -> list[Path]:
     if carb.exists():
         host.append(("libref_host_carb.so", ["-DREF_CARB", "-DUSE_DOUBLE", '-DREF_INC="_ref/carb_host.inc"'],
                      OUT / "carb_host.inc"))
+    if rec3.exists():
+        host.append(("libref_host_rec3.so", ["-DREF_REC3", "-Dreal=double", "-Dreall=double",
+                                             '-DREF_INC="_ref/rec3_host.inc"'], OUT / "rec3_host.inc"))
     built = []
     for name, defs, inc in host:
         out = OUT / name

@@ -9,6 +9,7 @@
  *   fvb_oracle_up7.h  : UP-ORDER + Ducros HLLC/HLLE path (fv_up7_ducros_2d.cu),
  *                       instantiated in float (as shipped) and double
  *   fvb_oracle_keep.h : ECKEP + JST/MOVERS-RH path (keep_fv_euler_2d.cu), double
+ *   fvb_oracle_rec3.h : rec3 + HLLC + 2x2-block Zhang-Shu path (fv_rec3_2d.cu), double
  */
 #include <math.h>
 #include <stddef.h>
@@ -46,6 +47,8 @@
 #include "fvb_oracle_up7.h"
 
 #include "fvb_oracle_keep.h"
+
+#include "fvb_oracle_rec3.h"
 
 /* ---- single-face entry points (unit tests of the Riemann solvers) ------- */
 void orc_hllc_f64(const double L[4], const double R[4], double F[4]) { hllc_f64(L, R, F); }

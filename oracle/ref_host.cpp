@@ -10,6 +10,7 @@
  *   -DREF_UP7 -DREF_REAL=double  its float->double retype
  *   -DREF_KEEP                   keep_fv_euler_2d.cu (FP64 already)
  *   -DREF_CARB -DUSE_DOUBLE      carb_fv_2d.cu's Riemann solvers, FP64
+ *   -DREF_REC3 -Dreal=double -Dreall=double   fv_rec3_2d.cu, FP64
  * Used to pin the oracle restatement bit-for-bit and as the CPU baseline
  * ("kind": "reference") of bench.py.
  */
@@ -170,6 +171,73 @@ extern "C" {
 void ref_carb_hllc(const real *WL, const real *WR, real nx, real ny, real *F) { hllc_n(WL, WR, nx, ny, F); }
 void ref_carb_hll(const real *WL, const real *WR, real nx, real ny, real *F) { hll_n(WL, WR, nx, ny, F); }
 void ref_carb_roe(const real *WL, const real *WR, real nx, real ny, real *F) { roe_n(WL, WR, nx, ny, F); }
+}  /* extern "C" */
+
+#elif defined(REF_REC3)
+/* fv_rec3_2d.cu built with real = reall = double */
+typedef double R;
+
+extern "C" {
+
+void ref_rec3_rhs(const R *Qp, R *RHS, R *lam, int N, int Np, R h)
+{
+    std::memset(RHS, 0, sizeof(R) * 4 * (size_t)N * N);
+    grid_launch((long long)N * N, [&] { compute_rhs(Qp, RHS, lam, N, Np, h); });
+}
+int ref_rec3_limit(R *Qp, int N, int Np)
+{
+    g_brutal_count = 0;
+    grid_launch((long long)(N / 2) * (N / 2), [&] { limit_positivity_blocks(Qp, N, Np); });
+    return g_brutal_count;
+}
+void ref_rec3_bc(R *Qp, int N, int Np) { grid_launch((long long)Np * Np, [&] { apply_bc(Qp, N, Np); }); }
+void ref_rec3_ic(R *Qp, int N, int Np, R h, int icase, R p0)
+{
+    std::memset(Qp, 0, sizeof(R) * 4 * (size_t)Np * Np);
+    grid_launch((long long)N * N, [&] { ic_kernel(Qp, N, Np, h, icase, p0); });
+}
+void ref_rec3_hllc(const R *WL, const R *WR, R nx, R ny, R *F) { hllc_n(WL, WR, nx, ny, F); }
+void ref_rec3_scale(const R *Ub, R *U) { scale_to_admissible(Ub, U); }
+
+/* the time loop of fv_rec3_2d.cu:551-590 around the kernels above, on a
+ * state that has had its limiter pass and ghost fill */
+int ref_rec3_run(R *U, int N, R h, R cfl, int max_steps, double t_stop, double *info)
+{
+    int Np = N + 2 * G_GHOST;
+    size_t nP = (size_t)4 * Np * Np, n1 = (size_t)N * N;
+    R *U0 = (R *)malloc(sizeof(R) * nP), *U1 = (R *)malloc(sizeof(R) * nP);
+    R *L = (R *)malloc(sizeof(R) * 4 * n1), *lam = (R *)malloc(sizeof(R) * n1);
+    std::memcpy(U1, U, sizeof(R) * nP);
+    ref_rec3_rhs(U, L, lam, N, Np, h);
+    R lmax = host_max(lam, (long long)n1), t = 0, dt = 0;
+    int step = 0, status = 0, brutal = 0;
+    while (step < max_steps && t < (R)t_stop) {
+        if (!(lmax > 0.)) { status = 1; break; }
+        dt = cfl * h / lmax;
+        if (t + dt > (R)t_stop) dt = (R)t_stop - t;
+        if (dt < 1e-14) { status = 2; break; }
+        std::memcpy(U0, U, sizeof(R) * nP);
+        grid_launch((long long)n1, [&] { rk_stage(U1, U0, U0, L, 0., 1., 0., dt, N, Np); });
+        brutal += ref_rec3_limit(U1, N, Np);
+        ref_rec3_bc(U1, N, Np);
+        ref_rec3_rhs(U1, L, lam, N, Np, h);
+        grid_launch((long long)n1, [&] { rk_stage(U1, U0, U1, L, 0.75, 0.25, 0., dt, N, Np); });
+        brutal += ref_rec3_limit(U1, N, Np);
+        ref_rec3_bc(U1, N, Np);
+        ref_rec3_rhs(U1, L, lam, N, Np, h);
+        grid_launch((long long)n1, [&] { rk_stage(U, U0, U1, L, (R)(1. / 3.), (R)(2. / 3.), 0., dt, N, Np); });
+        brutal += ref_rec3_limit(U, N, Np);
+        ref_rec3_bc(U, N, Np);
+        ref_rec3_rhs(U, L, lam, N, Np, h);
+        lmax = host_max(lam, (long long)n1);
+        t += dt;
+        step++;
+    }
+    if (info) { info[0] = t; info[1] = step; info[2] = lmax; info[3] = dt; info[4] = brutal; }
+    free(U0); free(U1); free(L); free(lam);
+    return status;
+}
+
 }  /* extern "C" */
 
 #elif defined(REF_KEEP)

@@ -24,3 +24,21 @@
 
 struct ref_dim3 { unsigned x, y, z; };
 extern thread_local ref_dim3 blockIdx, threadIdx, blockDim, gridDim;
+
+/* atomicAdd for kernels that scatter (fv_rec3_2d.cu's compute_rhs and its
+ * brutal-fix counter): an OpenMP atomic, so with one thread the additions
+ * happen in work-item order */
+inline double atomicAdd(double *a, double v)
+{
+    double old;
+#pragma omp atomic capture
+    { old = *a; *a += v; }
+    return old;
+}
+inline int atomicAdd(int *a, int v)
+{
+    int old;
+#pragma omp atomic capture
+    { old = *a; *a += v; }
+    return old;
+}

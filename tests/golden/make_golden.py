@@ -8,6 +8,7 @@ oracle restatement stays pinned where the reference checkout is absent.
 
     python tests/golden/make_golden.py          # every fixture
     python tests/golden/make_golden.py carb     # carb_fv's HLL / Roe faces only
+    python tests/golden/make_golden.py rec3     # those and fv_rec3's cases
 """
 from __future__ import annotations
 
@@ -75,14 +76,35 @@ def _faces_carb(seed=11, count=64):
     return out
 
 
+def _rec3():
+    """fv_rec3_2d.cu's own kernels (FP64, one host thread): initial states of
+    the Sod, paper-vortex and Gresho cases after the limiter and ghost fill,
+    their residuals, and 8 steps of each"""
+    out = {}
+    for case, N, L in (("sod", 16, 1.0), ("pv", 16, 10.0), ("lmv", 16, 1.0)):
+        h = L / N
+        p0 = O.rec3_p0(0.1) if case == "lmv" else 0.0
+        U = O.ref_rec3_ic(N, h, case, p0)
+        O.ref_rec3_limit(U, N)
+        O.ref_rec3_bc(U, N)
+        R, lam = O.ref_rec3_rhs(U, N, h)
+        U8 = U.copy()
+        info = O.ref_rec3_run(U8, N, h, 0.4, 8)
+        out.update({case + "_U0": U, case + "_rhs": R, case + "_lam": lam, case + "_U8": U8,
+                    case + "_info": np.array(info)})
+    return out
+
+
 def main() -> None:
     if not O.have_ref_host():
         raise SystemExit("oracle/_ref is not built (python oracle/build.py)")
+    O.ref_set_threads(1)  # scatter kernels add in work-item order
     if O.have_ref_carb():
         np.savez_compressed(HERE / "faces_carb_f64.npz", **_faces_carb())
-    if sys.argv[1:] == ["carb"]:
+    if O.have_ref_rec3():
+        np.savez_compressed(HERE / "rec3_16.npz", **_rec3())
+    if sys.argv[1:] in (["carb"], ["rec3"]):
         return
-    O.ref_set_threads(1)
     N = 16
     for dtype, sfx in ((np.float64, "f64"), (np.float32, "f32")):
         np.savez_compressed(HERE / ("faces_%s.npz" % sfx), **_faces(dtype))

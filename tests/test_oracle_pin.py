@@ -184,3 +184,90 @@ def test_riemann_variants_step_conserves_and_differs(riemann):
     assert abs(b[0] - a[0]) <= 1e-12 * abs(a[0]) and abs(b[3] - a[3]) <= 1e-12 * abs(a[3])
     d = np.abs(U - V).max()
     assert 1e-8 < d < 1e-1
+
+
+# --- fv_rec3_2d.cu: rec3 + HLLC + 2x2-block Zhang-Shu -------------------------
+
+def _rec3_case(case, N):
+    L = 10.0 if case == "pv" else 1.0
+    p0 = O.rec3_p0(0.1) if case == "lmv" else 0.0
+    return L / N, p0
+
+
+@pytest.mark.parametrize("case", ["sod", "pv", "lmv"])
+def test_rec3_golden(case):
+    z = np.load(GOLD / "rec3_16.npz")
+    N = 16
+    h, p0 = _rec3_case(case, N)
+    U = O.rec3_ic(N, h, case, p0)
+    O.rec3_limit(U, N)
+    O.bc(U, N, 2, 1)
+    assert np.array_equal(U, z[case + "_U0"])
+    R, lam = O.rec3_rhs(U, N, h)
+    assert np.array_equal(R, z[case + "_rhs"]) and np.array_equal(lam, z[case + "_lam"])
+    info = O.rec3_run(U, N, h, 0.4, 8)
+    assert np.array_equal(U, z[case + "_U8"])
+    assert np.array_equal(np.array(info), z[case + "_info"])
+
+
+def _rec3_stress(N):
+    """two strong rarefactions: near-vacuum that drives both positivity
+    limiters, the brutal mean fix and finally the dt-underflow guard"""
+    h = 1.0 / N
+    x = (np.arange(N) + 0.5) * h
+    X, Y = np.meshgrid(x, x)
+    rho = np.where(np.abs(X - 0.5) < 0.25, 1.0, 0.5)
+    u = np.where(X < 0.5, -3.0, 3.0)
+    v = 0.5 * np.sin(2 * np.pi * Y)
+    p = np.full_like(rho, 0.05)
+    U = np.zeros((4, N + 4, N + 4))
+    c = (slice(None), slice(2, -2), slice(2, -2))
+    U[c] = np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)])
+    return U
+
+
+needs_rec3 = pytest.mark.skipif(not O.have_ref_rec3(), reason="fv_rec3 host build absent")
+
+
+@needs_rec3
+@pytest.mark.parametrize("case,N", [("sod", 32), ("pv", 24), ("lmv", 20), ("stress", 32)])
+def test_rec3_oracle_matches_reference_host(case, N):
+    O.ref_set_threads(1)
+    if case == "stress":
+        h, p0 = 1.0 / N, 0.0
+        U = _rec3_stress(N)
+        V = U.copy()
+    else:
+        h, p0 = _rec3_case(case, N)
+        U = O.rec3_ic(N, h, case, p0)
+        V = O.ref_rec3_ic(N, h, case, p0)
+        assert np.array_equal(U, V)
+    assert O.rec3_limit(U, N) == O.ref_rec3_limit(V, N)
+    O.bc(U, N, 2, 1)
+    O.ref_rec3_bc(V, N)
+    assert np.array_equal(U, V)
+    ia = O.rec3_run(U, N, h, 0.4, 40)
+    ib = O.ref_rec3_run(V, N, h, 0.4, 40)
+    assert ia == ib
+    assert np.array_equal(U, V)
+    if case == "stress":
+        assert ia[0] == 2 and ia[5] > 0   # the reference scheme breaks down, with brutal fixes
+
+
+@needs_rec3
+def test_rec3_face_scaling_and_hllc_match_reference():
+    rng = np.random.default_rng(9)
+    sw = [0, 2, 1, 3]
+    for _ in range(300):
+        Ub = np.array([rng.uniform(0.1, 2), rng.uniform(-1, 1), rng.uniform(-1, 1), rng.uniform(1, 3)])
+        U = Ub + rng.normal(0, 1.5, 4)   # often inadmissible
+        a = O.rec3_scale(Ub, U)
+        b = U.copy()
+        O.ref_rec3("scale")(O._ptr(Ub), O._ptr(b))
+        assert np.array_equal(a, b)
+        wl = np.array([rng.uniform(0.1, 3), rng.uniform(-2, 2), rng.uniform(-2, 2), rng.uniform(0.1, 3)])
+        wr = np.array([rng.uniform(0.1, 3), rng.uniform(-2, 2), rng.uniform(-2, 2), rng.uniform(0.1, 3)])
+        for nx, ny, perm in ((1.0, 0.0, [0, 1, 2, 3]), (0.0, 1.0, sw)):
+            F = np.empty(4)
+            O.ref_rec3("hllc")(O._ptr(wl), O._ptr(wr), O.C.c_double(nx), O.C.c_double(ny), O._ptr(F))
+            assert np.array_equal(O.rec3_hllc(wl[perm], wr[perm])[perm], F)
