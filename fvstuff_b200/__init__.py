@@ -23,7 +23,7 @@ __all__ = ["Solver", "Stats", "FvbError", "case_params", "up_rhs", "apply_bc", "
 
 
 def ghost_width(order: int = 7, flux: str = "up_ducros") -> int:
-    return 2 if flux == "keep" else (order + 1) // 2
+    return 2 if flux in ("keep", "rec3") else (order + 1) // 2
 
 
 @dataclass
@@ -54,6 +54,7 @@ def case_params(kind: str, x0: float = 0.0, y0: float = 0.0, length: float = 1.0
         "kh": ["yc", "half_width", "rho_in", "rho_out", "u_in", "u_out", "p", "noise"],
         "riemann4": ["xm", "ym"],
         "lmv": ["eps"],
+        "gresho": ["eps"],
         "uniform": ["rho", "u", "v", "p"],
     }.get(kind, [])
     for k, v in overrides.items():

@@ -15,12 +15,13 @@ LIB_PATH = Path(os.environ.get("FVB_LIBRARY", Path(__file__).resolve().parent / 
 
 # enums (include/fvb.h)
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_BLOWUP, ERR_DT_UNDERFLOW, ERR_NOT_FOUND, ERR_TIMEOUT = range(8)
-FLUX = {"up_ducros": 0, "keep": 1, "up_ducros_hll": 2, "up_ducros_roe": 3}
+FLUX = {"up_ducros": 0, "keep": 1, "up_ducros_hll": 2, "up_ducros_roe": 3, "rec3": 4}
 PREC = {"f64": 0, "f32": 1, "f32c": 2}
 BC = {"reflect": 0, "periodic": 1, "transmissive": 2}
 LAYOUT = {"prim": 0, "cons": 1}
 DTYPE = {"f32": 0, "f64": 1}
-CASE = {"sod": 0, "vortex": 1, "kh": 2, "riemann4": 3, "keep_sod": 4, "lmv": 5, "uniform": 6}
+CASE = {"sod": 0, "vortex": 1, "kh": 2, "riemann4": 3, "keep_sod": 4, "lmv": 5, "uniform": 6, "rec3_sod": 7,
+        "paper_vortex": 8, "gresho": 9}
 
 
 class Config(C.Structure):

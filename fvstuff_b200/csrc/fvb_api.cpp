@@ -114,6 +114,9 @@ void case_defaults(fvb_case *c, int kind, double x0, double y0, double L)
     case FVB_CASE_UNIFORM:
         c->param[0] = 1.0; c->param[3] = 1.0;
         break;
+    case FVB_CASE_GRESHO:
+        c->param[0] = 0.1;  // eps (fv_rec3_2d.cu:511)
+        break;
     default:
         break;
     }
@@ -143,6 +146,7 @@ struct fvb_solver {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int graph_steps = 1;
     bool keep = false;  // KEEP flux family: conserved FP64 state, g = 2
+    bool rec3 = false;  // rec3 + Zhang-Shu family: conserved FP64 state, g = 2
     int rs = 0;         // solver on the reconstructed states: 0 HLLC, 1 HLL, 2 Roe
     // frame extraction (fvb_frame_begin / fvb_frame_end)
     float *frame_prim = nullptr;   // device, FP32 primitives with ghosts
@@ -178,9 +182,10 @@ static StageArgs stage_args(const fvb_solver *s, int stage, int parity)
 static cudaError_t enqueue_steps_direct(fvb_solver *s, int nsteps)
 {
     for (int k = 0; k < nsteps; ++k) {
-        if (s->keep) {
+        if (s->keep || s->rec3) {
             for (int stage = 1; stage <= 3; ++stage) {
-                cudaError_t e = keep_launch_stage(s->gd, stage, s->tiles, s->stream);
+                cudaError_t e = s->keep ? keep_launch_stage(s->gd, stage, s->tiles, s->stream)
+                                        : rec3_launch_stage(s->gd, stage, s->tiles, s->stream);
                 if (e != cudaSuccess) return e;
             }
             continue;
@@ -239,6 +244,15 @@ static fvb_status refresh_after_state(fvb_solver *s, int buf_parity)
 {
     cudaError_t e;
     BufView v = view_of(s->gd);
+    if (s->rec3) {
+        // as fv_rec3 after its initial state: the limiter pass, then ghosts
+        e = cudaMemsetAsync(&s->ctrl->aux, 0, sizeof(unsigned long long), s->stream);
+        if (e == cudaSuccess) e = rec3_limit_into(s->gd, s->gd.st[0], s->stream);
+        if (e == cudaSuccess) e = bc_fill<double>((double *)s->gd.st[0], v, s->gd.bcx, s->gd.bcy, s->stream);
+        if (e == cudaSuccess) e = rec3_lam_into(s->gd, s->stream);
+        if (e == cudaSuccess) e = ctrl_set(s->ctrl, 0.0, 1, 0.0, s->cfg.cfl, s->cfg.length / s->n, s->stream);
+        return e == cudaSuccess ? FVB_OK : cuda_fail(e, "state refresh");
+    }
     if (s->keep) {
         e = bc_fill<double>((double *)s->gd.st[0], v, s->gd.bcx, s->gd.bcy, s->stream);
         if (e == cudaSuccess) e = keep_lam_into(s->gd, s->stream);
@@ -294,19 +308,23 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     if (!cfg || !out) return fail(FVB_ERR_INVALID, "null argument");
     *out = nullptr;
     const bool keep = cfg->flux == FVB_FLUX_KEEP;
+    const bool rec3 = cfg->flux == FVB_FLUX_REC3;
     const int rs = cfg->flux == FVB_FLUX_UP_DUCROS_HLL ? 1 : cfg->flux == FVB_FLUX_UP_DUCROS_ROE ? 2 : 0;
-    if (cfg->flux != FVB_FLUX_UP_DUCROS && !keep && rs == 0)
+    if (cfg->flux != FVB_FLUX_UP_DUCROS && !keep && !rec3 && rs == 0)
         return fail(FVB_ERR_INVALID, "unknown flux %d", cfg->flux);
+    if (rec3 && (cfg->precision != FVB_PREC_F64 || cfg->bc_x != FVB_BC_PERIODIC || cfg->bc_y != FVB_BC_PERIODIC ||
+                 cfg->n % 2))
+        return fail(FVB_ERR_INVALID, "the rec3 family runs in FP64 on periodic grids of even n (as fv_rec3_2d.cu)");
     if (rs && !(cfg->precision == FVB_PREC_F64 && cfg->order == 7))
         return fail(FVB_ERR_INVALID, "the HLL / Roe variants are built for FP64, order 7");
     if (cfg->precision < 0 || cfg->precision > 2) return fail(FVB_ERR_INVALID, "unknown precision %d", cfg->precision);
     if (keep && cfg->precision != FVB_PREC_F64)
         return fail(FVB_ERR_INVALID, "the KEEP flux family runs in FP64 (as keep_fv_euler_2d.cu)");
-    if (!keep && !(cfg->order == 3 || cfg->order == 5 || cfg->order == 7))
+    if (!keep && !rec3 && !(cfg->order == 3 || cfg->order == 5 || cfg->order == 7))
         return fail(FVB_ERR_INVALID, "order must be 3, 5 or 7 (got %d)", cfg->order);
-    if (!keep && cfg->precision != FVB_PREC_F64 && cfg->order != 7)
+    if (!keep && !rec3 && cfg->precision != FVB_PREC_F64 && cfg->order != 7)
         return fail(FVB_ERR_INVALID, "orders 3 and 5 are built for FP64 only");
-    const int g = keep ? 2 : (cfg->order + 1) / 2;
+    const int g = (keep || rec3) ? 2 : (cfg->order + 1) / 2;
     if (cfg->n < g || cfg->n > 65536) return fail(FVB_ERR_INVALID, "n = %d out of range [%d, 65536]", cfg->n, g);
     for (int b : {cfg->bc_x, cfg->bc_y})
         if (b < 0 || b > 2) return fail(FVB_ERR_INVALID, "unknown boundary condition %d", b);
@@ -324,8 +342,9 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     s->g = g;
     s->n = cfg->n;
     s->keep = keep;
+    s->rec3 = rec3;
     s->rs = rs;
-    s->internal = keep ? INT_CONS64 : prec_internal(s->prec);
+    s->internal = (keep || rec3) ? INT_CONS64 : prec_internal(s->prec);
     s->G = make_geometry(cfg->n, g, s->prec);
     if (cfg->stream) s->stream = (cudaStream_t)cfg->stream;
     else {
@@ -355,9 +374,10 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     e = cudaMallocHost(&s->ctrl_host, sizeof(Ctrl));
     if (e != cudaSuccess) { fvb_destroy(s); return cuda_fail(e, "cudaMallocHost"); }
 
-    if (keep) {
-        // KEEP: plain loads into its own tile kernel, no graph variants
-        keep_tiles(s->n, s->gd.tiles_x, s->tiles);
+    if (keep || rec3) {
+        // KEEP / rec3: plain loads into their own tile kernels
+        if (keep) keep_tiles(s->n, s->gd.tiles_x, s->tiles);
+        else rec3_tiles(s->n, s->gd.tiles_x, s->tiles);
         s->graph_steps = 1;
         s->use_graph = cfg->n <= 512;
         e = ctrl_set(s->ctrl, 0.0, 1, 0.0, cfg->cfl, s->gd.h, s->stream);
@@ -421,6 +441,14 @@ int fvb_ghost_width(const fvb_solver *s) { return s ? s->g : 0; }
 fvb_status fvb_init_case(fvb_solver *s, const fvb_case *c)
 {
     if (!s || !c) return fail(FVB_ERR_INVALID, "null argument");
+    if (c->kind >= FVB_CASE_REC3_SOD && c->kind <= FVB_CASE_GRESHO) {
+        if (!s->rec3) return fail(FVB_ERR_INVALID, "case %d is a rec3 case (FVB_FLUX_REC3)", c->kind);
+        const double eps = c->param[0] > 0 ? c->param[0] : 0.1;
+        const double p0 = 1.0 / (s->cfg.gamma * eps * eps) - 0.5;  // fv_rec3_2d.cu:518
+        cudaError_t e = rec3_init_case(s->gd, c->kind - FVB_CASE_REC3_SOD, p0, s->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "initial state");
+        return refresh_after_state(s, 0);
+    }
     fvb_status st = ensure_staging(s);
     if (st) return st;
     cudaError_t e = init_case_prim64((double *)s->staging, s->n, s->cfg.x0, s->cfg.y0, s->gd.h, s->cfg.gamma, *c,

@@ -35,4 +35,13 @@ void keep_tiles(int n, int &tiles_x, int &tiles);
 cudaError_t keep_launch_stage(const GridDev &gd, int stage, int tiles, cudaStream_t s);
 cudaError_t keep_lam_into(const GridDev &gd, cudaStream_t s);
 
+// rec3 + HLLC + 2x2-block Zhang-Shu (fvb_rec3.cu): tiles, one fused stage,
+// the limiter pass over a whole state, max wave speed, fv_rec3's initial
+// states (0 Sod, 1 paper vortex, 2 Gresho with background pressure p0)
+void rec3_tiles(int n, int &tiles_x, int &tiles);
+cudaError_t rec3_launch_stage(const GridDev &gd, int stage, int tiles, cudaStream_t s);
+cudaError_t rec3_limit_into(const GridDev &gd, void *buf, cudaStream_t s);
+cudaError_t rec3_lam_into(const GridDev &gd, cudaStream_t s);
+cudaError_t rec3_init_case(const GridDev &gd, int icase, double p0, cudaStream_t s);
+
 }  // namespace fvb

@@ -48,7 +48,11 @@ typedef enum fvb_flux {
     /* UP7 + Ducros blend with carb_fv's alternatives to HLLC on the
      * reconstructed states (carb_fv_2d.cu:116-211; FP64, order 7) */
     FVB_FLUX_UP_DUCROS_HLL = 2,
-    FVB_FLUX_UP_DUCROS_ROE = 3
+    FVB_FLUX_UP_DUCROS_ROE = 3,
+    /* rec3 (kappa = 1/3) reconstruction of the conserved variables, face
+     * Zhang-Shu scaling, HLLC, 2x2-block Zhang-Shu positivity limiter after
+     * every stage (fv_rec3_2d.cu:147-353; FP64, periodic, N even) */
+    FVB_FLUX_REC3 = 4
 } fvb_flux;
 
 typedef enum fvb_precision {
@@ -79,7 +83,13 @@ typedef enum fvb_case_kind {
     FVB_CASE_RIEMANN4 = 3,    /* four-quadrant 2-D Riemann problem from a seed                    */
     FVB_CASE_KEEP_SOD = 4,    /* keep_fv circular Sod (keep_fv_euler_2d.cu:448-469)               */
     FVB_CASE_LMV = 5,         /* stationary low-Mach vortex (keep_fv_euler_2d.cu:471-513)         */
-    FVB_CASE_UNIFORM = 6      /* constant state (param[0..3] = rho, u, v, p)                      */
+    FVB_CASE_UNIFORM = 6,     /* constant state (param[0..3] = rho, u, v, p)                      */
+    /* fv_rec3_2d.cu's cases, as conserved cell averages (FVB_FLUX_REC3 only,
+     * fv_rec3_2d.cu:383-416): sharp circular Sod 10/0.125, the paper's
+     * isentropic vortex on [0,10]^2, the Gresho vortex (param[0] = eps) */
+    FVB_CASE_REC3_SOD = 7,
+    FVB_CASE_PAPER_VORTEX = 8,
+    FVB_CASE_GRESHO = 9
 } fvb_case_kind;
 
 /* One grid: N x N cells on [x0, x0 + length] x [y0, y0 + length], h = length / N. */
