@@ -174,6 +174,12 @@ class Solver:
         check(lib().fvb_get_state_hilo(self._h, hi.ctypes.data, lo.ctypes.data), "fvb_get_state_hilo")
         return hi, lo
 
+    def debug_drop_load(self) -> None:
+        """Failure injection: the next stage launch loses its first halo-box
+        load; its bounded wait runs out and the status becomes
+        FVB_ERR_TIMEOUT (see fvb_debug_drop_load)."""
+        check(lib().fvb_debug_drop_load(self._h), "fvb_debug_drop_load")
+
     # frames ------------------------------------------------------------------
     FRAME_FIELDS = ("rho", "vorticity", "ducros", "speed", "p")
 

@@ -79,6 +79,7 @@ _SIG = {
     "fvb_get_state": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int]),
     "fvb_get_state_hilo": (C.c_int, [_P, _P, _P]),
     "fvb_frame_begin": (C.c_int, [_P]),
+    "fvb_debug_drop_load": (C.c_int, [_P]),
     "fvb_frame_end": (C.c_int, [_P, _P]),
     "fvb_save": (C.c_int, [_P, C.c_char_p]),
     "fvb_load": (C.c_int, [_P, C.c_char_p]),

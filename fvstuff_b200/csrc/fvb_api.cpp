@@ -518,6 +518,16 @@ fvb_status fvb_get_state(fvb_solver *s, void *dst, int layout, int dtype, int wh
     return FVB_OK;
 }
 
+fvb_status fvb_debug_drop_load(fvb_solver *s)
+{
+    if (!s) return fail(FVB_ERR_INVALID, "null argument");
+    if (s->keep || s->rec3 || !s->gd.tmap) return fail(FVB_ERR_INVALID, "the hook needs a TMA-fed UP grid");
+    static const int one = 1;
+    cudaError_t e = cudaMemcpyAsync(&s->ctrl->drop_load, &one, sizeof one, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return e == cudaSuccess ? FVB_OK : cuda_fail(e, "arm");
+}
+
 // ---- frames: extraction on the device, copy on a second stream ----------
 
 fvb_status fvb_frame_begin(fvb_solver *s)

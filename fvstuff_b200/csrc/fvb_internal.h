@@ -29,8 +29,10 @@ struct Ctrl {
     int active;                 // the step in progress runs
     int status;                 // fvb_status of the step control
     int clamped;                // dt was clamped to land on t_stop
-    int pad;
-    unsigned long long aux;     // KEEP: bit pattern of the entropy-distance max of the stage input
+    int drop_load;              // failure-injection hook: the next single-grid stage launch
+                                // issues no first halo-box load (its wait must run out)
+    unsigned long long aux;     // KEEP: bit pattern of the entropy-distance max of the stage
+                                // input; rec3: count of 2x2 blocks given the brutal mean fix
 };
 
 // Device view of one grid.  Element (q, jp, ip) of a padded buffer, padded

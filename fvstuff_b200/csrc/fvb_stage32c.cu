@@ -81,6 +81,12 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
         issue_tile_load<P32C, G, SW, SH, NT>(a.grid, a.stage, cur, t, IN, &s_bar, tid);
         return a.grid.tmap != nullptr;
     };
+    // failure injection (fvb_debug_drop_load): CTA 0 of a single-grid launch
+    // issues no first box load, so its bounded wait runs out and the grid's
+    // status becomes FVB_ERR_TIMEOUT; the flag is read by every thread of
+    // that CTA before thread 0 clears it behind the first barrier
+    const bool drop = !batched && blockIdx.x == 0 && a.stage > 0 && a.grid.ctrl && a.grid.tmap &&
+                      *(volatile int *)&a.grid.ctrl->drop_load;
     const int stride = gridDim.x;
     int t = blockIdx.x, slot = 0;
     if (t < ntiles && batched) {
@@ -90,6 +96,9 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
             if (tid == 0 && t + stride < ntiles) s_ref_next = a.tiles[t + stride];
         }
         wait_box(true);
+    } else if (drop) {
+        wait_box(true);  // nothing was issued: the wait runs out
+        if (tid == 0) a.grid.ctrl->drop_load = 0;
     } else {
         wait_box(t < ntiles ? start_single(t) : false);
     }

@@ -45,10 +45,20 @@ __device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *map, int
         : "memory");
 }
 
-// bounded wait for phase `parity` of `bar`; false when the limit ran out
+// bounded wait for phase `parity` of `bar`: false once one second of GPU
+// time (%globaltimer) has passed without the phase completing
+__device__ __forceinline__ uint64_t gtimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 {
-    for (uint32_t it = 0; it < (1u << 24); ++it) {
+    constexpr uint64_t kLimitNs = 1000000000ull;
+    uint64_t t0 = 0;
+    for (uint32_t it = 0;; ++it) {
         uint32_t ok;
         asm volatile(
             "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
@@ -56,8 +66,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
             : "r"(smem_u32(bar)), "r"(parity)
             : "memory");
         if (ok) return true;
+        if ((it & 63) == 0) {
+            const uint64_t now = gtimer_ns();
+            if (it == 0) t0 = now;
+            else if (now - t0 > kLimitNs) return false;
+        }
     }
-    return false;
 }
 
 // The halo box of a tile in one grid: TMA when the grid has descriptors,

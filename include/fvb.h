@@ -190,6 +190,14 @@ FVB_API fvb_status fvb_step(fvb_solver *s, int nsteps, double t_stop);
 FVB_API fvb_status fvb_advance(fvb_solver *s, double t_stop, int64_t max_steps, int chunk);
 /* Wait for the stream and read the step control (t, dt, lam_max, status). */
 FVB_API fvb_status fvb_sync(fvb_solver *s, fvb_stats *st);
+
+/* Failure injection for tests (no counterpart in the reference): the next
+ * stage launch of this solver issues no first halo-box load on its first
+ * CTA, so that CTA's bounded wait (one second of GPU time) runs out, the
+ * kernel ends normally and the solver's status becomes FVB_ERR_TIMEOUT --
+ * the path a lost asynchronous copy would take.  The GPU context stays
+ * usable; the solver stops stepping, as after a blow-up. */
+FVB_API fvb_status fvb_debug_drop_load(fvb_solver *s);
 /* As fvb_sync, plus FP64 conserved sums over the interior. */
 FVB_API fvb_status fvb_stats_sums(fvb_solver *s, fvb_stats *st);
 /* Record the whole step (three stage kernels) as a CUDA graph and replay it
