@@ -93,7 +93,12 @@ __device__ __forceinline__ bool gd_has_tma(const StageArgs &a)
     return a.grids != nullptr || a.grid.tmap != nullptr;
 }
 
-// Step control, evaluated by thread 0 of each CTA for its tile's grid.
+// Step control of one grid for one stage.  `leader` (one thread of the
+// launch per grid: thread 0 of CTA 0 of a single-grid launch, the
+// stage-control kernel's thread for a batch, thread 0 of the tile-0 CTA of
+// the KEEP and rec3 kernels) also writes the stage's control updates: dt,
+// `active` and `clamped` in stage 1, the wave-speed accumulator reset in
+// stage 2.  Every other caller only reads.
 template <int PREC>
 __device__ TileCtl tile_control(Ctrl *c, int stage, bool leader)
 {

@@ -1,4 +1,7 @@
-// fvb_stage.cu -- the fused SSP-RK3 stage kernel.
+// fvb_stage.cu -- the fused SSP-RK3 stage kernel of the FP64 plain method
+// (and of the FP32 form as shipped), the step-control kernel of batched
+// launches, the tile-variant tables and the TMA descriptors.  The FP32-
+// compensated form has its own kernel (fvb_stage32c.cu).
 //
 // One launch = one RK stage of one grid (or of every grid of a batch, through
 // a tile table).  Per tile of TX x TY interior cells a CTA
