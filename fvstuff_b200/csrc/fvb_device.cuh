@@ -73,6 +73,37 @@ __device__ __forceinline__ void put_cell(const GridDev &gd, R *buf, int j, int i
     }
 }
 
+// Store two cell values that share a layout (the hi and lo words of the
+// compensated state) into the interior and all their ghost images.
+template <class R>
+__device__ __forceinline__ void put_cell2(const GridDev &gd, R *bufA, R *bufB, int j, int i, const R va[4],
+                                          const R vb[4])
+{
+    const long long pl = gd.plane;
+    const long long c = gidx(gd, 0, j, i);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        bufA[c + q * pl] = va[q];
+        bufB[c + q * pl] = vb[q];
+    }
+    const int g = gd.g, n = gd.n;
+    if (i >= g && i < n - g && j >= g && j < n - g) return;
+    const int nx = n_images(i, n, g, gd.bcx), ny = n_images(j, n, g, gd.bcy);
+    for (int ka = 0; ka < ny; ++ka) {
+        bool fy;
+        const int y = image_of(ka, j, n, g, gd.bcy, fy);
+        for (int kb = (ka == 0 ? 1 : 0); kb < nx; ++kb) {
+            bool fx;
+            const int x = image_of(kb, i, n, g, gd.bcx, fx);
+            const long long e = gidx(gd, 0, y, x);
+            bufA[e] = va[0]; bufB[e] = vb[0];
+            bufA[e + pl] = fx ? -va[1] : va[1]; bufB[e + pl] = fx ? -vb[1] : vb[1];
+            bufA[e + 2 * pl] = fy ? -va[2] : va[2]; bufB[e + 2 * pl] = fy ? -vb[2] : vb[2];
+            bufA[e + 3 * pl] = va[3]; bufB[e + 3 * pl] = vb[3];
+        }
+    }
+}
+
 // Error-free sum of a double-float (hi, lo) and a float increment d
 // (Knuth TwoSum for hi + d, then Dekker FastTwoSum to renormalise).
 __device__ __forceinline__ void df_add(float &hi, float &lo, float d)

@@ -103,6 +103,19 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
         wait_box(t < ntiles ? start_single(t) : false);
     }
     double lacc = 0.0;
+    // which of this thread's conversion cells (k = tid + it NT) the HLLE
+    // reads the sound speed and energy of: the interior rows x columns
+    // [G-1, G+TX], and rows G-1, G+TY x the interior columns
+    constexpr int NCV = (PL + NT - 1) / NT;
+    static_assert(NCV <= 32, "one mask bit per conversion cell");
+    unsigned cemask = 0;
+#pragma unroll
+    for (int it = 0; it < NCV; ++it) {
+        const int k = tid + it * NT, r = k / SW, c = k - r * SW;
+        const bool ce = ((unsigned)(r - G) < (unsigned)TY && (unsigned)(c - (G - 1)) < (unsigned)(TX + 2)) ||
+                        ((r == G - 1 || r == G + TY) && (unsigned)(c - G) < (unsigned)TX);
+        cemask |= (ce && k < PL ? 1u : 0u) << it;
+    }
     // one grid: the step control is the same for every tile of the launch,
     // read once (the leader is CTA 0, whose first tile is tile 0)
     TileCtl ctl1{};
@@ -131,17 +144,17 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
             break;
         }
         // ---- 1. stage input U0 + d into W as primitives (+ c, E where the
-        //         HLLE reads them: interior rows x columns [G-1, G+TX], and
-        //         rows G-1, G+TY x the interior columns) --------------------
+        //         HLLE reads them, cemask) ------------------------------------
         if (ctl.run) {
-            for (int k = tid; k < PL; k += NT) {
+#pragma unroll
+            for (int it = 0; it < NCV; ++it) {
+                const int k = tid + it * NT;
+                if (k >= PL) break;
                 float w0 = IN[k], w1 = IN[PL + k], w2 = IN[2 * PL + k], w3 = IN[3 * PL + k];
                 if (a.stage >= 2) {
                     w0 += IN[4 * PL + k]; w1 += IN[5 * PL + k]; w2 += IN[6 * PL + k]; w3 += IN[7 * PL + k];
                 }
-                const int r = k / SW, c = k - r * SW;
-                const bool ce = ((unsigned)(r - G) < (unsigned)TY && (unsigned)(c - (G - 1)) < (unsigned)(TX + 2)) ||
-                                ((r == G - 1 || r == G + TY) && (unsigned)(c - G) < (unsigned)TX);
+                const bool ce = (cemask >> it) & 1u;
                 const float ir = frcp(w0);
                 const float E = w3;
                 w1 *= ir;
@@ -181,8 +194,7 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
                     float vh[4], vl[4];
                     long long e = gidx(gd, 0, j, i);
                     for (int q = 0; q < 4; ++q) { vh[q] = hi[e + q * gd.plane]; vl[q] = lo[e + q * gd.plane]; }
-                    put_cell<float>(gd, (float *)gd.st[nxt], j, i, vh);
-                    put_cell<float>(gd, (float *)gd.lo[nxt], j, i, vl);
+                    put_cell2<float>(gd, (float *)gd.st[nxt], (float *)gd.lo[nxt], j, i, vh, vl);
                 }
             }
             wait_box(next_tma);
@@ -278,8 +290,7 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
                     float ke = 0.5f * (vh[1] * vh[1] + vh[2] * vh[2]) / vh[0];
                     vh[3] = 1e-14f / gm1 + ke; vl[3] = 0.f; w[3] = 1e-14f;
                 }
-                put_cell<float>(gd, (float *)gd.st[nxt], j, i, vh);
-                put_cell<float>(gd, (float *)gd.lo[nxt], j, i, vl);
+                put_cell2<float>(gd, (float *)gd.st[nxt], (float *)gd.lo[nxt], j, i, vh, vl);
                 float cs2 = gam * w[3] * frcp(w[0]);
                 float lam = fabsf(w[1]) + fabsf(w[2]) + fsqrt(cs2 > 1e-14f ? cs2 : 1e-14f);
                 lmax = fmax(lmax, (double)lam);
