@@ -23,7 +23,11 @@ __all__ = ["Solver", "Stats", "FvbError", "case_params", "up_rhs", "apply_bc", "
 
 
 def ghost_width(order: int = 7, flux: str = "up_ducros") -> int:
-    return 2 if flux in ("keep", "rec3") else (order + 1) // 2
+    if flux in ("keep", "rec3"):
+        return 2
+    if flux == "up_hllc_d2av":  # the velocity-divergence sensor reaches 3 cells
+        return max((order + 1) // 2, 3)
+    return (order + 1) // 2
 
 
 @dataclass
@@ -92,7 +96,8 @@ class Solver:
 
     Parameters mirror fvb_config: ``n`` cells per side on
     ``[x0, x0+length] x [y0, y0+length]``, ``order`` (3/5/7), ``flux``
-    ('up_ducros' | 'keep'), ``precision`` ('f64' | 'f32' | 'f32c'),
+    ('up_ducros' | 'up_ducros_hll' | 'up_ducros_roe' | 'keep' | 'rec3' |
+    'up_hllc_d2av'), ``precision`` ('f64' | 'f32' | 'f32c'),
     ``bc`` / ``bc_y`` ('reflect' | 'periodic' | 'transmissive'), ``gamma``,
     ``cfl``.  Defaults are those of fv_up7_ducros_2d.cu (UP7, reflecting
     walls, unit square, CFL 0.4) with FP64 arithmetic.
@@ -179,6 +184,11 @@ class Solver:
         load; its bounded wait runs out and the status becomes
         FVB_ERR_TIMEOUT (see fvb_debug_drop_load)."""
         check(lib().fvb_debug_drop_load(self._h), "fvb_debug_drop_load")
+
+    def set_d2av(self, c2: float = 0.5, cg: float = 0.0, sc: float = 0.05) -> None:
+        """Coefficients of the 'up_hllc_d2av' viscosity (the .bak solver's
+        C2, Cg and sc arguments; see fvb_set_d2av)."""
+        check(lib().fvb_set_d2av(self._h, c2, cg, sc), "fvb_set_d2av")
 
     # frames ------------------------------------------------------------------
     FRAME_FIELDS = ("rho", "vorticity", "ducros", "speed", "p")

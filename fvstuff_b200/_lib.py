@@ -15,7 +15,7 @@ LIB_PATH = Path(os.environ.get("FVB_LIBRARY", Path(__file__).resolve().parent / 
 
 # enums (include/fvb.h)
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_BLOWUP, ERR_DT_UNDERFLOW, ERR_NOT_FOUND, ERR_TIMEOUT = range(8)
-FLUX = {"up_ducros": 0, "keep": 1, "up_ducros_hll": 2, "up_ducros_roe": 3, "rec3": 4}
+FLUX = {"up_ducros": 0, "keep": 1, "up_ducros_hll": 2, "up_ducros_roe": 3, "rec3": 4, "up_hllc_d2av": 5}
 PREC = {"f64": 0, "f32": 1, "f32c": 2}
 BC = {"reflect": 0, "periodic": 1, "transmissive": 2}
 LAYOUT = {"prim": 0, "cons": 1}
@@ -80,6 +80,7 @@ _SIG = {
     "fvb_get_state_hilo": (C.c_int, [_P, _P, _P]),
     "fvb_frame_begin": (C.c_int, [_P]),
     "fvb_debug_drop_load": (C.c_int, [_P]),
+    "fvb_set_d2av": (C.c_int, [_P, C.c_double, C.c_double, C.c_double]),
     "fvb_frame_end": (C.c_int, [_P, _P]),
     "fvb_save": (C.c_int, [_P, C.c_char_p]),
     "fvb_load": (C.c_int, [_P, C.c_char_p]),

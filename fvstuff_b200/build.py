@@ -26,9 +26,10 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
          "-I", str(ROOT / "include"), "-I", str(CSRC), "--expt-relaxed-constexpr"]
 
 
-# per-file flags: the rec3 kernels reproduce the reference's arithmetic
-# operation for operation, so no multiply-add contraction there
-FILE_FLAGS = {"fvb_rec3.cu": ["-fmad=false"]}
+# per-file flags: the rec3 and D2-viscosity kernels reproduce the
+# reference's arithmetic operation for operation, so no multiply-add
+# contraction there
+FILE_FLAGS = {"fvb_rec3.cu": ["-fmad=false"], "fvb_d2av.cu": ["-fmad=false"]}
 
 
 def _run(cmd):

@@ -147,6 +147,8 @@ struct fvb_solver {
     int graph_steps = 1;
     bool keep = false;  // KEEP flux family: conserved FP64 state, g = 2
     bool rec3 = false;  // rec3 + Zhang-Shu family: conserved FP64 state, g = 2
+    bool d2av = false;  // UP + HLLC + D2 viscosity (.bak): conserved FP64 state, g >= 3
+    D2Params av{0.5, 0.0, 0.05};  // its C2, Cg, sc (fv_up7_ducros_2d.cu.bak:742-744)
     int rs = 0;         // solver on the reconstructed states: 0 HLLC, 1 HLL, 2 Roe
     // frame extraction (fvb_frame_begin / fvb_frame_end)
     float *frame_prim = nullptr;   // device, FP32 primitives with ghosts
@@ -182,10 +184,11 @@ static StageArgs stage_args(const fvb_solver *s, int stage, int parity)
 static cudaError_t enqueue_steps_direct(fvb_solver *s, int nsteps)
 {
     for (int k = 0; k < nsteps; ++k) {
-        if (s->keep || s->rec3) {
+        if (s->keep || s->rec3 || s->d2av) {
             for (int stage = 1; stage <= 3; ++stage) {
-                cudaError_t e = s->keep ? keep_launch_stage(s->gd, stage, s->tiles, s->stream)
-                                        : rec3_launch_stage(s->gd, stage, s->tiles, s->stream);
+                cudaError_t e = s->keep   ? keep_launch_stage(s->gd, stage, s->tiles, s->stream)
+                                : s->rec3 ? rec3_launch_stage(s->gd, stage, s->tiles, s->stream)
+                                          : d2av_launch_stage(s->gd, s->order, stage, s->tiles, s->av, s->stream);
                 if (e != cudaSuccess) return e;
             }
             continue;
@@ -253,9 +256,9 @@ static fvb_status refresh_after_state(fvb_solver *s, int buf_parity)
         if (e == cudaSuccess) e = ctrl_set(s->ctrl, 0.0, 1, 0.0, s->cfg.cfl, s->cfg.length / s->n, s->stream);
         return e == cudaSuccess ? FVB_OK : cuda_fail(e, "state refresh");
     }
-    if (s->keep) {
+    if (s->keep || s->d2av) {
         e = bc_fill<double>((double *)s->gd.st[0], v, s->gd.bcx, s->gd.bcy, s->stream);
-        if (e == cudaSuccess) e = keep_lam_into(s->gd, s->stream);
+        if (e == cudaSuccess) e = s->keep ? keep_lam_into(s->gd, s->stream) : d2av_lam_into(s->gd, s->stream);
         if (e == cudaSuccess) e = ctrl_set(s->ctrl, 0.0, 1, 0.0, s->cfg.cfl, s->cfg.length / s->n, s->stream);
         return e == cudaSuccess ? FVB_OK : cuda_fail(e, "state refresh");
     }
@@ -309,9 +312,12 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     *out = nullptr;
     const bool keep = cfg->flux == FVB_FLUX_KEEP;
     const bool rec3 = cfg->flux == FVB_FLUX_REC3;
+    const bool d2av = cfg->flux == FVB_FLUX_UP_HLLC_D2AV;
     const int rs = cfg->flux == FVB_FLUX_UP_DUCROS_HLL ? 1 : cfg->flux == FVB_FLUX_UP_DUCROS_ROE ? 2 : 0;
-    if (cfg->flux != FVB_FLUX_UP_DUCROS && !keep && !rec3 && rs == 0)
+    if (cfg->flux != FVB_FLUX_UP_DUCROS && !keep && !rec3 && !d2av && rs == 0)
         return fail(FVB_ERR_INVALID, "unknown flux %d", cfg->flux);
+    if (d2av && cfg->precision != FVB_PREC_F64)
+        return fail(FVB_ERR_INVALID, "the UP + HLLC + D2 viscosity scheme runs in FP64 (as fv_up7_ducros_2d.cu.bak)");
     if (rec3 && (cfg->precision != FVB_PREC_F64 || cfg->bc_x != FVB_BC_PERIODIC || cfg->bc_y != FVB_BC_PERIODIC ||
                  cfg->n % 2))
         return fail(FVB_ERR_INVALID, "the rec3 family runs in FP64 on periodic grids of even n (as fv_rec3_2d.cu)");
@@ -324,7 +330,7 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
         return fail(FVB_ERR_INVALID, "order must be 3, 5 or 7 (got %d)", cfg->order);
     if (!keep && !rec3 && cfg->precision != FVB_PREC_F64 && cfg->order != 7)
         return fail(FVB_ERR_INVALID, "orders 3 and 5 are built for FP64 only");
-    const int g = (keep || rec3) ? 2 : (cfg->order + 1) / 2;
+    const int g = (keep || rec3) ? 2 : d2av ? d2av_ghost(cfg->order) : (cfg->order + 1) / 2;
     if (cfg->n < g || cfg->n > 65536) return fail(FVB_ERR_INVALID, "n = %d out of range [%d, 65536]", cfg->n, g);
     for (int b : {cfg->bc_x, cfg->bc_y})
         if (b < 0 || b > 2) return fail(FVB_ERR_INVALID, "unknown boundary condition %d", b);
@@ -343,8 +349,9 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     s->n = cfg->n;
     s->keep = keep;
     s->rec3 = rec3;
+    s->d2av = d2av;
     s->rs = rs;
-    s->internal = (keep || rec3) ? INT_CONS64 : prec_internal(s->prec);
+    s->internal = (keep || rec3 || d2av) ? INT_CONS64 : prec_internal(s->prec);
     s->G = make_geometry(cfg->n, g, s->prec);
     if (cfg->stream) s->stream = (cudaStream_t)cfg->stream;
     else {
@@ -374,10 +381,11 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     e = cudaMallocHost(&s->ctrl_host, sizeof(Ctrl));
     if (e != cudaSuccess) { fvb_destroy(s); return cuda_fail(e, "cudaMallocHost"); }
 
-    if (keep || rec3) {
-        // KEEP / rec3: plain loads into their own tile kernels
+    if (keep || rec3 || d2av) {
+        // KEEP / rec3 / D2 viscosity: plain loads into their own tile kernels
         if (keep) keep_tiles(s->n, s->gd.tiles_x, s->tiles);
-        else rec3_tiles(s->n, s->gd.tiles_x, s->tiles);
+        else if (rec3) rec3_tiles(s->n, s->gd.tiles_x, s->tiles);
+        else d2av_tiles(s->n, s->gd.tiles_x, s->tiles);
         s->graph_steps = 1;
         s->use_graph = cfg->n <= 512;
         e = ctrl_set(s->ctrl, 0.0, 1, 0.0, cfg->cfl, s->gd.h, s->stream);
@@ -518,10 +526,21 @@ fvb_status fvb_get_state(fvb_solver *s, void *dst, int layout, int dtype, int wh
     return FVB_OK;
 }
 
+fvb_status fvb_set_d2av(fvb_solver *s, double c2, double cg, double sc)
+{
+    if (!s) return fail(FVB_ERR_INVALID, "null argument");
+    if (!s->d2av) return fail(FVB_ERR_INVALID, "the solver does not use FVB_FLUX_UP_HLLC_D2AV");
+    if (!(c2 >= 0) || !(cg >= 0) || !(sc >= 0)) return fail(FVB_ERR_INVALID, "C2, Cg and sc must be >= 0");
+    s->av = D2Params{c2, cg, sc};
+    drop_graphs(s);  // the kernels take the coefficients as arguments
+    return FVB_OK;
+}
+
 fvb_status fvb_debug_drop_load(fvb_solver *s)
 {
     if (!s) return fail(FVB_ERR_INVALID, "null argument");
-    if (s->keep || s->rec3 || !s->gd.tmap) return fail(FVB_ERR_INVALID, "the hook needs a TMA-fed UP grid");
+    if (s->keep || s->rec3 || s->d2av || !s->gd.tmap)
+        return fail(FVB_ERR_INVALID, "the hook needs a TMA-fed UP grid");
     static const int one = 1;
     cudaError_t e = cudaMemcpyAsync(&s->ctrl->drop_load, &one, sizeof one, cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -552,6 +571,8 @@ fvb_status fvb_frame_begin(fvb_solver *s)
         e = export_state(s->gd.st[s->internal == INT_CONS_HILO ? p : 0], s->gd.lo[p], view_of(s->gd), s->internal,
                          s->frame_prim, ev, s->cfg.gamma, s->stream);
     if (e == cudaSuccess) e = frame_fields(s->frame_prim, s->n, s->g, s->G.np, s->gd.h, s->frame_dev, s->stream);
+    // the .bak scheme's sensor panel is its own velocity-divergence weight
+    if (e == cudaSuccess && s->d2av) e = d2av_sensor_into(s->gd, s->av.sc, s->frame_dev + 2 * n2, s->stream);
     if (e == cudaSuccess) e = cudaEventRecord(s->frame_ready, s->stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copy_stream, s->frame_ready, 0);
     if (e == cudaSuccess)

@@ -19,6 +19,13 @@ struct ExtView {
     int dtype;   // fvb_dtype
 };
 
+// coefficients of the D2 artificial viscosity of the .bak scheme
+// (fv_up7_ducros_2d.cu.bak:742-745): Ducros-gated C2, global Cg, sensor
+// sound-speed scale sc
+struct D2Params {
+    double c2, cg, sc;
+};
+
 // internal state kinds
 enum { INT_PRIM64 = 0, INT_PRIM32 = 1, INT_CONS_HILO = 2, INT_CONS64 = 3 };
 

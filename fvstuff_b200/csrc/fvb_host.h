@@ -44,4 +44,15 @@ cudaError_t rec3_limit_into(const GridDev &gd, void *buf, cudaStream_t s);
 cudaError_t rec3_lam_into(const GridDev &gd, cudaStream_t s);
 cudaError_t rec3_init_case(const GridDev &gd, int icase, double p0, cudaStream_t s);
 
+// UP + HLLC + Ducros-gated D2 viscosity of fv_up7_ducros_2d.cu.bak
+// (fvb_d2av.cu): ghost width of an order (the sensor reaches 3 cells), tiles,
+// one fused stage, the wave-speed max of a state, and the Ducros weight of
+// every cell as FP32 (frames)
+int d2av_ghost(int order);
+void d2av_tiles(int n, int &tiles_x, int &tiles);
+cudaError_t d2av_launch_stage(const GridDev &gd, int order, int stage, int tiles, const D2Params &av,
+                              cudaStream_t s);
+cudaError_t d2av_lam_into(const GridDev &gd, cudaStream_t s);
+cudaError_t d2av_sensor_into(const GridDev &gd, double sc, float *out, cudaStream_t s);
+
 }  // namespace fvb

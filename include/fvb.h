@@ -52,7 +52,13 @@ typedef enum fvb_flux {
     /* rec3 (kappa = 1/3) reconstruction of the conserved variables, face
      * Zhang-Shu scaling, HLLC, 2x2-block Zhang-Shu positivity limiter after
      * every stage (fv_rec3_2d.cu:147-353; FP64, periodic, N even) */
-    FVB_FLUX_REC3 = 4
+    FVB_FLUX_REC3 = 4,
+    /* the scheme kept in fv_up7_ducros_2d.cu.bak: UP-order reconstruction of
+     * the conserved variables, HLLC, and a D2 artificial viscosity gated by
+     * a Ducros weight from the 6th-order velocity divergence
+     * (fv_up7_ducros_2d.cu.bak:287-390; FP64, order 3, 5 or 7, ghost width
+     * max((order + 1) / 2, 3); coefficients from fvb_set_d2av) */
+    FVB_FLUX_UP_HLLC_D2AV = 5
 } fvb_flux;
 
 typedef enum fvb_precision {
@@ -190,6 +196,12 @@ FVB_API fvb_status fvb_step(fvb_solver *s, int nsteps, double t_stop);
 FVB_API fvb_status fvb_advance(fvb_solver *s, double t_stop, int64_t max_steps, int chunk);
 /* Wait for the stream and read the step control (t, dt, lam_max, status). */
 FVB_API fvb_status fvb_sync(fvb_solver *s, fvb_stats *st);
+
+/* Coefficients of the FVB_FLUX_UP_HLLC_D2AV viscosity: C2 (Ducros-gated),
+ * Cg (global, weight 1 - S_D) and the sensor's sound-speed scale sc; the
+ * .bak's command-line arguments 2-4, defaults 0.5, 0, 0.05
+ * (fv_up7_ducros_2d.cu.bak:742-744).  FVB_ERR_INVALID for other fluxes. */
+FVB_API fvb_status fvb_set_d2av(fvb_solver *s, double c2, double cg, double sc);
 
 /* Failure injection for tests (no counterpart in the reference): the next
  * stage launch of this solver issues no first halo-box load on its first

@@ -252,6 +252,93 @@ def ref_rec3_run(U, N, h, cfl, max_steps, t_stop=1e30):
     return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3]), int(info[4])
 
 
+# ---- fv_up7_ducros_2d.cu.bak: UP + HLLC + Ducros-gated D2 viscosity (FP64) -
+def d2av_ghost(order: int = 5) -> int:
+    return max((order + 1) // 2, 3)
+
+
+def d2av_ic_sod(N: int, h: float, order: int = 5) -> np.ndarray:
+    """The .bak's circular Sod, conserved, padded (ghosts not filled)."""
+    g = d2av_ghost(order)
+    U = padded(N, g)
+    lib().orc_d2av_ic_sod(_ptr(U), C.c_int(N), C.c_double(h), C.c_int(g))
+    return U
+
+
+def d2av_rhs(Q: np.ndarray, N: int, h: float, order: int = 5, c2: float = 0.5, cg: float = 0.0,
+             sc: float = 0.05):
+    """Residual (4,N,N) and lam (N,N) of a padded conserved state with its ghosts filled."""
+    g = d2av_ghost(order)
+    assert Q.shape == (4, N + 2 * g, N + 2 * g) and Q.flags.c_contiguous and Q.dtype == np.float64
+    R = np.empty((4, N, N)); lam = np.empty((N, N))
+    lib().orc_d2av_rhs(_ptr(Q), _ptr(R), _ptr(lam), C.c_int(N), C.c_int(order), C.c_double(h), C.c_double(c2),
+                       C.c_double(cg), C.c_double(sc))
+    return R, lam
+
+
+def d2av_sensor(Q: np.ndarray, N: int, h: float, order: int = 5, sc: float = 0.05) -> np.ndarray:
+    SD = np.empty((N, N))
+    lib().orc_d2av_sensor(_ptr(Q), _ptr(SD), C.c_int(N), C.c_int(order), C.c_double(h), C.c_double(sc))
+    return SD
+
+
+def d2av_run(U: np.ndarray, N: int, h: float, cfl: float, bc_kind: int, max_steps: int, t_stop: float = 1e30,
+             order: int = 5, c2: float = 0.5, cg: float = 0.0, sc: float = 0.05):
+    """Advance U (padded conserved, ghosts filled) in place; returns
+    (status, t, steps, lam_max, last_dt)."""
+    info = np.zeros(4)
+    st = lib().orc_d2av_run(_ptr(U), C.c_int(N), C.c_int(order), C.c_int(bc_kind), C.c_double(h),
+                            C.c_double(cfl), C.c_double(c2), C.c_double(cg), C.c_double(sc), C.c_int(max_steps),
+                            C.c_double(t_stop), _ptr(info))
+    return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3])
+
+
+def d2av_hllc(UL, UR):
+    """The .bak's HLLC on conserved states, normal frame (rho, m_n, m_t, E)."""
+    UL, UR = np.ascontiguousarray(UL, np.float64), np.ascontiguousarray(UR, np.float64)
+    F = np.empty(4)
+    lib().orc_d2av_hllc(_ptr(UL), _ptr(UR), _ptr(F))
+    return F
+
+
+def have_ref_bak() -> bool:
+    return (REF / "libref_host_bak.so").exists()
+
+
+def ref_bak_rhs(U: np.ndarray, N: int, h: float, order: int = 5, c2: float = 0.5, cg: float = 0.0,
+                sc: float = 0.05):
+    """The .bak's own compute_rhs (host build) on an unpadded (4,N,N) conserved state."""
+    U = np.ascontiguousarray(U, np.float64)
+    R = np.empty((4, N, N)); lam = np.empty((N, N))
+    ref_host("bak").ref_bak_rhs(_ptr(U), _ptr(R), _ptr(lam), C.c_int(N), C.c_double(h), C.c_double(c2),
+                                C.c_double(cg), C.c_double(sc), C.c_int(order))
+    return R, lam
+
+
+def ref_bak_sensor(U: np.ndarray, N: int, h: float, sc: float = 0.05) -> np.ndarray:
+    U = np.ascontiguousarray(U, np.float64)
+    SD = np.empty((N, N))
+    ref_host("bak").ref_bak_sensor(_ptr(U), _ptr(SD), C.c_int(N), C.c_double(h), C.c_double(sc))
+    return SD
+
+
+def ref_bak_ic(N: int, h: float) -> np.ndarray:
+    U = np.zeros((4, N, N))
+    ref_host("bak").ref_bak_ic(_ptr(U), C.c_int(N), C.c_double(h))
+    return U
+
+
+def ref_bak_run(U: np.ndarray, N: int, h: float, cfl: float, max_steps: int, t_stop: float = 1e30,
+                order: int = 5, c2: float = 0.5, cg: float = 0.0, sc: float = 0.05):
+    """The .bak's kernels in its time loop (reflecting walls), unpadded U in place."""
+    info = np.zeros(4)
+    f = ref_host("bak").ref_bak_run
+    f.restype = C.c_int
+    st = f(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(cfl), C.c_double(c2), C.c_double(cg), C.c_double(sc),
+           C.c_int(order), C.c_int(max_steps), C.c_double(t_stop), _ptr(info))
+    return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3])
+
+
 def hlle(L, R, dtype=np.float64):
     L = np.ascontiguousarray(L, dtype); R = np.ascontiguousarray(R, dtype); F = np.empty(4, dtype)
     getattr(lib(), "orc_hlle_" + _sfx(dtype))(_ptr(L), _ptr(R), _ptr(F))
@@ -300,7 +387,7 @@ def keep_err_lmv(U: np.ndarray, N: int, h: float, eps: float = 0.1):
 # the reference's own kernels, host build (oracle/_ref/libref_host_*.so)
 # ---------------------------------------------------------------------------
 def ref_set_threads(n: int) -> None:
-    for k in ("up7_f32", "up7_f64", "keep", "carb", "rec3"):
+    for k in ("up7_f32", "up7_f64", "keep", "carb", "rec3", "bak"):
         try:
             ref_host(k).ref_set_threads(C.c_int(n))
         except FileNotFoundError:
@@ -394,6 +481,24 @@ def refg_keep_run(U: np.ndarray, N: int, h: float, cfl: float, max_steps: int, t
     ms = C.c_float(0)
     st = ref_gpu("keep").refg_keep_run(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(cfl), C.c_int(max_steps),
                                        C.c_double(t_stop), _ptr(info), C.byref(ms))
+    if st > 0:
+        raise RuntimeError("reference GPU run failed: cuda error %d" % st)
+    return -int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3]), float(ms.value)
+
+
+def have_ref_gpu_bak() -> bool:
+    return (REF / "libref_gpu_bak.so").exists()
+
+
+def refg_bak_run(U: np.ndarray, N: int, h: float, cfl: float, max_steps: int, t_stop: float = 1e30,
+                 order: int = 5, c2: float = 0.5, cg: float = 0.0, sc: float = 0.05):
+    """The .bak's kernels and loop on the GPU (unpadded U in place);
+    (status, t, steps, lam_max, last_dt, ms of the stepping loop)."""
+    info = np.zeros(4)
+    ms = C.c_float(0)
+    st = ref_gpu("bak").refg_bak_run(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(cfl), C.c_double(c2),
+                                     C.c_double(cg), C.c_double(sc), C.c_int(order), C.c_int(max_steps),
+                                     C.c_double(t_stop), _ptr(info), C.byref(ms))
     if st > 0:
         raise RuntimeError("reference GPU run failed: cuda error %d" % st)
     return -int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3]), float(ms.value)

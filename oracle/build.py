@@ -47,6 +47,11 @@ REC3 = "fv_rec3_2d.cu"
 # constants and floors, then everything from IDX_P to the error kernel;
 # left out: includes, the CK() macro, the reductions, host code and main
 REC3_HOST_LINES = [(36, 60), (65, 447)]
+BAK = "fv_up7_ducros_2d.cu.bak"
+# GAMMA_V, IDX, then everything from the fetch helper to the RK3 kernels,
+# and the IC kernel; left out: includes, CK(), the reductions, image output
+# and main
+BAK_HOST_LINES = [(27, 27), (43, 446), (469, 491)]
 
 NVCC = os.environ.get("NVCC", "nvcc")
 GPU_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -96,7 +101,7 @@ def _write_if_changed(p: Path, text: str) -> None:
 def build_oracle(verbose: bool = False) -> Path:
     out = HERE / "liboracle.so"
     deps = [HERE / "fvb_oracle.c", HERE / "fvb_oracle_up7.h", HERE / "fvb_oracle_keep.h",
-            HERE / "fvb_oracle_rec3.h", HERE / "build.py"]
+            HERE / "fvb_oracle_rec3.h", HERE / "fvb_oracle_d2av.h", HERE / "build.py"]
     if _stale(out, deps):
         _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off",
               "-o", str(out), str(HERE / "fvb_oracle.c"), "-lm"])
@@ -121,6 +126,9 @@ def build_ref(verbose: bool = False, gpu: bool = True) -> list[Path]:
     rec3 = REF_DIR / REC3
     if rec3.exists():
         _write_if_changed(OUT / "rec3_host.inc", _extract(rec3, REC3_HOST_LINES))
+    bak = REF_DIR / BAK
+    if bak.exists():
+        _write_if_changed(OUT / "bak_host.inc", _extract(bak, BAK_HOST_LINES))
     _write_if_changed(OUT / "fv_up7_f64.cu", retype_f64(up7_text))
 
     host_flags = ["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared",
@@ -138,6 +146,8 @@ def build_ref(verbose: bool = False, gpu: bool = True) -> list[Path]:
     if rec3.exists():
         host.append(("libref_host_rec3.so", ["-DREF_REC3", "-Dreal=double", "-Dreall=double",
                                              '-DREF_INC="_ref/rec3_host.inc"'], OUT / "rec3_host.inc"))
+    if bak.exists():
+        host.append(("libref_host_bak.so", ["-DREF_BAK", '-DREF_INC="_ref/bak_host.inc"'], OUT / "bak_host.inc"))
     built = []
     for name, defs, inc in host:
         out = OUT / name
@@ -157,6 +167,8 @@ def build_ref(verbose: bool = False, gpu: bool = True) -> list[Path]:
                                        '-DREF_CU="_ref/fv_up7_f64.cu"'], OUT / "fv_up7_f64.cu"),
             ("libref_gpu_keep.so", ["-DREF_KEEP", '-DREF_CU="%s"' % keep], keep),
         ]
+        if bak.exists():
+            dev.append(("libref_gpu_bak.so", ["-DREF_BAK", '-DREF_CU="%s"' % bak], bak))
         for name, defs, src in dev:
             out = OUT / name
             if _stale(out, [src, HERE / "ref_gpu.cu", HERE / "build.py"]):

@@ -10,6 +10,8 @@
  *                       instantiated in float (as shipped) and double
  *   fvb_oracle_keep.h : ECKEP + JST/MOVERS-RH path (keep_fv_euler_2d.cu), double
  *   fvb_oracle_rec3.h : rec3 + HLLC + 2x2-block Zhang-Shu path (fv_rec3_2d.cu), double
+ *   fvb_oracle_d2av.h : UP + HLLC + Ducros-gated D2 viscosity path
+ *                       (fv_up7_ducros_2d.cu.bak), double
  */
 #include <math.h>
 #include <stddef.h>
@@ -50,6 +52,8 @@
 
 #include "fvb_oracle_rec3.h"
 
+#include "fvb_oracle_d2av.h"
+
 /* ---- single-face entry points (unit tests of the Riemann solvers) ------- */
 void orc_hllc_f64(const double L[4], const double R[4], double F[4]) { hllc_f64(L, R, F); }
 void orc_hlle_f64(const double L[4], const double R[4], double F[4]) { hlle_f64(L, R, F); }
@@ -59,3 +63,4 @@ void orc_hll_f64(const double L[4], const double R[4], double F[4]) { hll_f64(L,
 void orc_roe_f64(const double L[4], const double R[4], double F[4]) { roe_f64(L, R, F); }
 void orc_upface_f64(int order, const double *s, double *vL, double *vR) { upface_f64(order, s, vL, vR); }
 void orc_upface_f32(int order, const float *s, float *vL, float *vR) { upface_f32(order, s, vL, vR); }
+void orc_d2av_hllc(const double L[4], const double R[4], double F[4]) { d2_hllc(L, R, F); }

@@ -222,4 +222,62 @@ int refg_keep_run(R *Uh, int N, R h, R cfl, int max_steps, double t_stop, double
 }
 
 }  /* extern "C" */
+
+#elif defined(REF_BAK)
+typedef double R;
+
+extern "C" {
+
+/* the time loop of fv_up7_ducros_2d.cu.bak:848-872 with its kernels and
+ * launches (unpadded N x N conserved state, reflecting fetch), stopping at
+ * max_steps or t_stop; ms_out: CUDA-event time of the stepping loop */
+int refg_bak_run(R *Uh, int N, R h, R cfl, R C2, R Cg, R sc, int order, int max_steps, double t_stop,
+                 double *info, float *ms_out)
+{
+    size_t sz4 = (size_t)4 * N * N * sizeof(R), n1 = (size_t)N * N;
+    int M = 4 * N * N;
+    R *dU, *dU0, *dU1, *dU2, *dRHS, *dlam, *dtmp;
+    RET_ON_ERR(cudaMalloc(&dU, sz4)); RET_ON_ERR(cudaMalloc(&dU0, sz4));
+    RET_ON_ERR(cudaMalloc(&dU1, sz4)); RET_ON_ERR(cudaMalloc(&dU2, sz4));
+    RET_ON_ERR(cudaMalloc(&dRHS, sz4));
+    RET_ON_ERR(cudaMalloc(&dlam, n1 * sizeof(R)));
+    RET_ON_ERR(cudaMalloc(&dtmp, GS_NBLK * sizeof(R)));
+    RET_ON_ERR(cudaMemcpy(dU, Uh, sz4, cudaMemcpyHostToDevice));
+    RET_ON_ERR(cudaDeviceSynchronize());
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    R t = 0, dt = 0, lmax = 0;
+    int step = 0, status = 0;
+    while (step < max_steps && t < t_stop) {
+        compute_rhs<<<GS_NBLK, BLOCK1D>>>(dU, dRHS, dlam, N, h, C2, Cg, sc, order);
+        lmax = gpu_max(dlam, dtmp, N * N);
+        if (!(lmax > 0.)) { status = 1; break; }
+        dt = cfl * h / lmax;
+        if (t + dt > t_stop) dt = t_stop - t;
+        if (dt < 1e-14) { status = 2; break; }
+        RET_ON_ERR(cudaMemcpy(dU0, dU, sz4, cudaMemcpyDeviceToDevice));
+        rk3_s1<<<GS_NBLK, BLOCK1D>>>(dU1, dU0, dRHS, dt, M);
+        compute_rhs<<<GS_NBLK, BLOCK1D>>>(dU1, dRHS, dlam, N, h, C2, Cg, sc, order);
+        rk3_s2<<<GS_NBLK, BLOCK1D>>>(dU2, dU0, dU1, dRHS, dt, M);
+        compute_rhs<<<GS_NBLK, BLOCK1D>>>(dU2, dRHS, dlam, N, h, C2, Cg, sc, order);
+        rk3_s3<<<GS_NBLK, BLOCK1D>>>(dU, dU0, dU2, dRHS, dt, M);
+        t += dt;
+        step++;
+    }
+    cudaEventRecord(e1);
+    RET_ON_ERR(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms_out) *ms_out = ms;
+    RET_ON_ERR(cudaGetLastError());
+    RET_ON_ERR(cudaMemcpy(Uh, dU, sz4, cudaMemcpyDeviceToHost));
+    if (info) { info[0] = t; info[1] = step; info[2] = lmax; info[3] = dt; }
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    cudaFree(dU); cudaFree(dU0); cudaFree(dU1); cudaFree(dU2);
+    cudaFree(dRHS); cudaFree(dlam); cudaFree(dtmp);
+    return status ? -status : 0;
+}
+
+}  /* extern "C" */
 #endif

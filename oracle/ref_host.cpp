@@ -11,6 +11,7 @@
  *   -DREF_KEEP                   keep_fv_euler_2d.cu (FP64 already)
  *   -DREF_CARB -DUSE_DOUBLE      carb_fv_2d.cu's Riemann solvers, FP64
  *   -DREF_REC3 -Dreal=double -Dreall=double   fv_rec3_2d.cu, FP64
+ *   -DREF_BAK                    fv_up7_ducros_2d.cu.bak (FP64 already)
  * Used to pin the oracle restatement bit-for-bit and as the CPU baseline
  * ("kind": "reference") of bench.py.
  */
@@ -235,6 +236,69 @@ int ref_rec3_run(R *U, int N, R h, R cfl, int max_steps, double t_stop, double *
     }
     if (info) { info[0] = t; info[1] = step; info[2] = lmax; info[3] = dt; info[4] = brutal; }
     free(U0); free(U1); free(L); free(lam);
+    return status;
+}
+
+}  /* extern "C" */
+
+#elif defined(REF_BAK)
+/* fv_up7_ducros_2d.cu.bak: unpadded N x N conserved state read through its
+ * reflecting fetch */
+typedef double R;
+
+extern "C" {
+
+void ref_bak_rhs(const R *U, R *RHS, R *lam, int N, R h, R C2, R Cg, R sc, int order)
+{
+    grid_launch((long long)N * N, [&] { compute_rhs(U, RHS, lam, N, h, C2, Cg, sc, order); });
+}
+void ref_bak_sensor(const R *U, R *SD, int N, R h, R sc)
+{
+    grid_launch((long long)N * N, [&] { compute_sensor(U, SD, N, h, sc); });
+}
+void ref_bak_rk3(int stage, R *Uo, const R *U0, const R *Uk, const R *L, R dt, int N)
+{
+    int M = 4 * N * N;
+    if (stage == 1) grid_launch(M, [&] { rk3_s1(Uo, U0, L, dt, M); });
+    else if (stage == 2) grid_launch(M, [&] { rk3_s2(Uo, U0, Uk, L, dt, M); });
+    else grid_launch(M, [&] { rk3_s3(Uo, U0, Uk, L, dt, M); });
+}
+void ref_bak_ic(R *U, int N, R h) { grid_launch((long long)N * N, [&] { ic_kernel(U, N, h); }); }
+void ref_bak_hllc(const R *UL, const R *UR, int yface, R *F)
+{
+    if (yface) hllc_y(UL, UR, F);
+    else hllc_x(UL, UR, F);
+}
+
+/* the time loop of fv_up7_ducros_2d.cu.bak:848-872 (residual and lam at
+ * the start of a step, dt = CFL h / lam_max clamped onto t_stop, stop on
+ * dt < 1e-14), with the stop on a non-positive lam_max of this library */
+int ref_bak_run(R *U, int N, R h, R cfl, R C2, R Cg, R sc, int order, int max_steps, double t_stop, double *info)
+{
+    size_t n4 = (size_t)4 * N * N, n1 = (size_t)N * N;
+    R *U0 = (R *)malloc(sizeof(R) * n4), *U1 = (R *)malloc(sizeof(R) * n4);
+    R *U2 = (R *)malloc(sizeof(R) * n4), *L = (R *)malloc(sizeof(R) * n4), *lam = (R *)malloc(sizeof(R) * n1);
+    ref_bak_rhs(U, L, lam, N, h, C2, Cg, sc, order);
+    R lmax = host_max(lam, (long long)n1), t = 0, dt = 0;
+    int step = 0, status = 0;
+    while (step < max_steps && t < t_stop) {
+        if (!(lmax > 0.)) { status = 1; break; }
+        dt = cfl * h / lmax;
+        if (t + dt > t_stop) dt = t_stop - t;
+        if (dt < 1e-14) { status = 2; break; }
+        memcpy(U0, U, sizeof(R) * n4);
+        ref_bak_rk3(1, U1, U0, U0, L, dt, N);
+        ref_bak_rhs(U1, L, lam, N, h, C2, Cg, sc, order);
+        ref_bak_rk3(2, U2, U0, U1, L, dt, N);
+        ref_bak_rhs(U2, L, lam, N, h, C2, Cg, sc, order);
+        ref_bak_rk3(3, U, U0, U2, L, dt, N);
+        ref_bak_rhs(U, L, lam, N, h, C2, Cg, sc, order);
+        lmax = host_max(lam, (long long)n1);
+        t += dt;
+        step++;
+    }
+    if (info) { info[0] = t; info[1] = step; info[2] = lmax; info[3] = dt; }
+    free(U0); free(U1); free(U2); free(L); free(lam);
     return status;
 }
 

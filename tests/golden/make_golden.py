@@ -9,6 +9,7 @@ oracle restatement stays pinned where the reference checkout is absent.
     python tests/golden/make_golden.py          # every fixture
     python tests/golden/make_golden.py carb     # carb_fv's HLL / Roe faces only
     python tests/golden/make_golden.py rec3     # those and fv_rec3's cases
+    python tests/golden/make_golden.py bak      # those and the .bak scheme's cases
 """
 from __future__ import annotations
 
@@ -95,6 +96,36 @@ def _rec3():
     return out
 
 
+def bak_state(N, seed):
+    """The .bak's circular Sod with a seeded velocity field and the kinetic
+    energy added (so every term of the scheme is exercised), unpadded."""
+    U = O.ref_bak_ic(N, 1.0 / N)
+    rng = np.random.default_rng(seed)
+    U[1] = U[0] * rng.uniform(-0.5, 0.5, (N, N))
+    U[2] = U[0] * rng.uniform(-0.5, 0.5, (N, N))
+    U[3] += 0.5 * (U[1] ** 2 + U[2] ** 2) / U[0]
+    return U
+
+
+def _bak():
+    """fv_up7_ducros_2d.cu.bak's own kernels (FP64): its circular Sod, the
+    residual, lam and sensor of a seeded state for orders 3/5/7 with both
+    viscosity terms on, and 6 steps of each from the Sod state"""
+    out = {}
+    N = 16
+    h = 1.0 / N
+    out["ic"] = O.ref_bak_ic(N, h)
+    for order in (3, 5, 7):
+        U = bak_state(N, order)
+        R, lam = O.ref_bak_rhs(U, N, h, order, 0.5, 0.02, 0.05)
+        out.update({"o%d_U" % order: U, "o%d_rhs" % order: R, "o%d_lam" % order: lam,
+                    "o%d_sd" % order: O.ref_bak_sensor(U, N, h, 0.05)})
+        U6 = out["ic"].copy()
+        info = O.ref_bak_run(U6, N, h, 0.4, 6, 1e30, order, 0.5, 0.02, 0.05)
+        out.update({"o%d_U6" % order: U6, "o%d_info" % order: np.array(info)})
+    return out
+
+
 def main() -> None:
     if not O.have_ref_host():
         raise SystemExit("oracle/_ref is not built (python oracle/build.py)")
@@ -103,7 +134,9 @@ def main() -> None:
         np.savez_compressed(HERE / "faces_carb_f64.npz", **_faces_carb())
     if O.have_ref_rec3():
         np.savez_compressed(HERE / "rec3_16.npz", **_rec3())
-    if sys.argv[1:] in (["carb"], ["rec3"]):
+    if O.have_ref_bak():
+        np.savez_compressed(HERE / "bak_16.npz", **_bak())
+    if sys.argv[1:] in (["carb"], ["rec3"], ["bak"]):
         return
     N = 16
     for dtype, sfx in ((np.float64, "f64"), (np.float32, "f32")):

@@ -271,3 +271,72 @@ def test_rec3_face_scaling_and_hllc_match_reference():
             F = np.empty(4)
             O.ref_rec3("hllc")(O._ptr(wl), O._ptr(wr), O.C.c_double(nx), O.C.c_double(ny), O._ptr(F))
             assert np.array_equal(O.rec3_hllc(wl[perm], wr[perm])[perm], F)
+
+
+# --- fv_up7_ducros_2d.cu.bak: UP + HLLC + Ducros-gated D2 viscosity -----------
+def _bak_padded(U, N, order, bc=0):
+    g = O.d2av_ghost(order)
+    Q = O.padded(N, g)
+    Q[:, g:g + N, g:g + N] = U
+    O.bc(Q, N, g, bc)
+    return Q, g
+
+
+@pytest.mark.parametrize("order", [3, 5, 7])
+def test_bak_golden(order):
+    z = np.load(GOLD / "bak_16.npz")
+    N = 16
+    h = 1.0 / N
+    g = O.d2av_ghost(order)
+    assert np.array_equal(O.d2av_ic_sod(N, h, order)[:, g:-g, g:-g], z["ic"])
+    Q, g = _bak_padded(z["o%d_U" % order], N, order)
+    R, lam = O.d2av_rhs(Q, N, h, order, 0.5, 0.02, 0.05)
+    assert np.array_equal(R, z["o%d_rhs" % order])
+    assert np.array_equal(lam, z["o%d_lam" % order])
+    assert np.array_equal(O.d2av_sensor(Q, N, h, order, 0.05), z["o%d_sd" % order])
+    Q, g = _bak_padded(z["ic"], N, order)
+    info = O.d2av_run(Q, N, h, 0.4, 0, 6, 1e30, order, 0.5, 0.02, 0.05)
+    assert np.array_equal(np.array(info), z["o%d_info" % order])
+    assert np.array_equal(Q[:, g:-g, g:-g], z["o%d_U6" % order])
+
+
+needs_bak = pytest.mark.skipif(not O.have_ref_bak(), reason="fv_up7_ducros_2d.cu.bak host build absent")
+
+
+@needs_bak
+@pytest.mark.parametrize("order,N,cg", [(3, 20, 0.0), (5, 33, 0.01), (7, 41, 0.0), (9, 24, 0.0)])
+def test_bak_oracle_matches_reference_host(order, N, cg):
+    """Ragged sizes, every order the .bak takes (UP9 with its published
+    weights), both viscosity terms, 12 steps through the reference's loop."""
+    O.ref_set_threads(1)
+    from golden.make_golden import bak_state
+    h = 1.0 / N
+    U = bak_state(N, 100 + order)
+    Q, g = _bak_padded(U, N, order)
+    R, lam = O.d2av_rhs(Q, N, h, order, 0.5, cg, 0.05)
+    Rr, lamr = O.ref_bak_rhs(U, N, h, order, 0.5, cg, 0.05)
+    assert np.array_equal(R, Rr) and np.array_equal(lam, lamr)
+    assert np.array_equal(O.d2av_sensor(Q, N, h, order, 0.05), O.ref_bak_sensor(U, N, h, 0.05))
+    V = O.ref_bak_ic(N, h)
+    Q, g = _bak_padded(V, N, order)
+    ia = O.d2av_run(Q, N, h, 0.4, 0, 12, 1e30, order, 0.5, cg, 0.05)
+    ib = O.ref_bak_run(V, N, h, 0.4, 12, 1e30, order, 0.5, cg, 0.05)
+    assert ia == ib and ia[0] == 0 and ia[2] == 12
+    assert np.array_equal(Q[:, g:-g, g:-g], V)
+
+
+@needs_bak
+def test_bak_hllc_matches_reference():
+    rng = np.random.default_rng(21)
+    sw = [0, 2, 1, 3]
+    f = O.ref_host("bak").ref_bak_hllc
+    for _ in range(400):
+        U = []
+        for _side in range(2):
+            r = rng.uniform(0.1, 3)
+            u, v, p = rng.uniform(-3, 3), rng.uniform(-3, 3), rng.uniform(0.1, 5)
+            U.append(np.array([r, r * u, r * v, p / 0.4 + 0.5 * r * (u * u + v * v)]))
+        for yface, perm in ((0, [0, 1, 2, 3]), (1, sw)):
+            F = np.empty(4)
+            f(O._ptr(U[0]), O._ptr(U[1]), O.C.c_int(yface), O._ptr(F))
+            assert np.array_equal(O.d2av_hllc(U[0][perm], U[1][perm])[perm], F)
