@@ -5,11 +5,18 @@
 //           [--gamma G] [--bc reflect|periodic|transmissive] [--order 3|5|7]
 //           [--precision f64|f32|f32c] [--frames F] [--prefix P] [--seed S]
 //           [--bin] [--no-ppm] [--save FILE] [--resume FILE]
+//   fvb_up7 --d2av [N [C2 [Cg [sc [order]]]]] [options above]
 //
 // Defaults are the reference's: N = 400, CFL 0.40, t_end 1, circular Sod
 // with reflecting walls on [0,1]^2, UP7 (FP64 arithmetic here), 10 frames
 // written as <prefix>_%04d.ppm (2N x 2N composite: density, vorticity,
 // Ducros sensor, |v|), frame 99 on blow-up.
+//
+// --d2av runs the scheme kept in fv_up7_ducros_2d.cu.bak instead (UP-order
+// reconstruction of the conserved variables, HLLC, Ducros-gated D2
+// viscosity), with that file's positional arguments (:741-745: N, C2, Cg,
+// sc, order; defaults 400, 0.5, 0, 0.05, 5), its Sod (density 10 inside)
+// and its composite, whose sensor panel is the velocity-divergence weight.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -29,6 +36,8 @@ struct Args {
     long long seed = -1;
     std::string prefix = "sod", save, resume;
     bool bin = false, ppm = true;
+    bool d2av = false;
+    double c2 = 0.5, cg = 0.0, sc = 0.05;
 };
 
 int parse_enum(const char *v, const char *const *names, int count, const char *what)
@@ -45,6 +54,9 @@ Args parse(int argc, char **argv)
     static const char *bcs[] = {"reflect", "periodic", "transmissive"};
     static const char *precs[] = {"f64", "f32", "f32c"};
     Args a;
+    for (int k = 1; k < argc; ++k)
+        if (!std::strcmp(argv[k], "--d2av")) { a.d2av = true; a.order = 5; }
+    int npos = 0;
     for (int k = 1; k < argc; ++k) {
         std::string s = argv[k];
         auto val = [&]() -> const char * {
@@ -65,7 +77,19 @@ Args parse(int argc, char **argv)
         else if (s == "--no-ppm") a.ppm = false;
         else if (s == "--save") a.save = val();
         else if (s == "--resume") a.resume = val();
-        else if (s[0] != '-') a.n = std::atoi(s.c_str());
+        else if (s == "--d2av") continue;
+        else if (s[0] != '-' && !a.d2av) a.n = std::atoi(s.c_str());
+        else if (s[0] != '-') {
+            // the .bak's positional arguments  fv_up7_ducros_2d.cu.bak:741-745
+            switch (npos++) {
+            case 0: a.n = std::atoi(s.c_str()); break;
+            case 1: a.c2 = std::atof(s.c_str()); break;
+            case 2: a.cg = std::atof(s.c_str()); break;
+            case 3: a.sc = std::atof(s.c_str()); break;
+            case 4: a.order = std::atoi(s.c_str()); break;
+            default: std::fprintf(stderr, "too many arguments\n"); std::exit(2);
+            }
+        }
         else { std::fprintf(stderr, "unknown option %s\n", s.c_str()); std::exit(2); }
     }
     if (a.bc < 0) a.bc = (a.kase == FVB_CASE_SOD) ? FVB_BC_REFLECT : (a.kase == FVB_CASE_RIEMANN4 ? FVB_BC_TRANSMISSIVE : FVB_BC_PERIODIC);
@@ -129,24 +153,34 @@ int main(int argc, char **argv)
     fvb_config_default(&cfg, a.n);
     cfg.order = a.order;
     cfg.precision = a.precision;
+    if (a.d2av) cfg.flux = FVB_FLUX_UP_HLLC_D2AV;
     cfg.bc_x = cfg.bc_y = a.bc;
     cfg.cfl = a.cfl;
     cfg.gamma = a.gamma;
     if (a.kase == FVB_CASE_VORTEX) { cfg.x0 = cfg.y0 = -5.0; cfg.length = 10.0; }
     fvb_solver *s = nullptr;
     if (fvb_create(&cfg, &s)) { std::fprintf(stderr, "fvb_create: %s\n", fvb_last_error()); return 1; }
+    if (a.d2av && fvb_set_d2av(s, a.c2, a.cg, a.sc)) {
+        std::fprintf(stderr, "fvb_set_d2av: %s\n", fvb_last_error());
+        return 1;
+    }
     const int g = fvb_ghost_width(s);
     const double h = cfg.length / a.n;
     static const char *names[] = {"Circular Sod", "Isentropic vortex", "Kelvin-Helmholtz", "Four-quadrant Riemann"};
     std::printf("========================================================\n");
     std::printf("  Device  : %s\n", fvb_version());
     std::printf("  UP%d+HLLC+Ducros FV 2D  --  %s\n", a.order, names[a.kase]);
-    std::printf("  n=%dx%d  Np=%d  h=%.5f  CFL=%.2f  order=%d\n", a.n, a.n, a.n + 2 * g, h, a.cfl, a.order);
+    if (a.d2av)
+        std::printf("  n=%dx%d  h=%.5f  C2=%.3f  Cg=%.4f  sc=%.4f  CFL=%.2f  order=%d\n", a.n, a.n, h, a.c2, a.cg, a.sc,
+                    a.cfl, a.order);
+    else
+        std::printf("  n=%dx%d  Np=%d  h=%.5f  CFL=%.2f  order=%d\n", a.n, a.n, a.n + 2 * g, h, a.cfl, a.order);
     std::printf("========================================================\n");
 
     fvb_case c;
     fvb_case_default(&c, a.kase, cfg.x0, cfg.y0, cfg.length);
     if (a.seed >= 0) c.seed = (uint64_t)a.seed;
+    if (a.d2av && a.kase == FVB_CASE_SOD) c.param[4] = 10.0;  // fv_up7_ducros_2d.cu.bak:484
     if (fvb_init_case(s, &c)) { std::fprintf(stderr, "init: %s\n", fvb_last_error()); return 1; }
     Frames F(a.n);
     // density colour scale fixed to the initial extremes for the whole run

@@ -47,6 +47,29 @@ def _png(path):
     return w, h
 
 
+def test_fvb_up7_d2av_frames(tmp_path):
+    """--d2av: the .bak's positional arguments (N C2 Cg sc order) and its
+    composite; the state written at the end equals a library run"""
+    r = subprocess.run([str(BIN / "fvb_up7"), "--d2av", "48", "0.6", "0.01", "0.05", "3", "--t-end", "0.02",
+                        "--frames", "2", "--save", "end.ckpt"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert "C2=0.600" in r.stdout and "order=3" in r.stdout and "frame  2/2" in r.stdout
+    for k in range(3):
+        w, h, img = _ppm(tmp_path / ("sod_%04d.ppm" % k))
+        assert (w, h) == (96, 96)
+    s = F.Solver(48, order=3, flux="up_hllc_d2av")
+    s.set_d2av(0.6, 0.01, 0.05)
+    s.init_case("sod", rho_in=10.0)
+    s.advance(0.01)
+    s.advance(0.02)
+    want = s.get_state(layout="cons", interior=True)
+    c = F.Solver(48, order=3, flux="up_hllc_d2av")
+    c.load(str(tmp_path / "end.ckpt"))
+    assert abs(c.sync().t - 0.02) < 1e-15
+    assert np.array_equal(c.get_state(layout="cons", interior=True), want)
+
+
 def test_fvb_up7_frames(tmp_path):
     r = subprocess.run([str(BIN / "fvb_up7"), "48", "--t-end", "0.02", "--frames", "2", "--bin"], cwd=tmp_path,
                        capture_output=True, text=True, timeout=120)
