@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
             continue;
         }
         const float dt = (float)ctl.dt;
-        const float inv_h = (float)(1.0 / gd.h);
+        const float dt_h = dt * (float)(1.0 / gd.h);
 
         // ---- 3. face fluxes, x-face p and y-face p as one packed pair -------
         for (int p = tid; p < NP; p += NT) {
@@ -244,28 +244,25 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
         __syncthreads();
 
         // ---- 4. divergence, RK combination, stores --------------------------
-        double lmax = 0.0;
+        float lmax = 0.0f;
         for (int k = tid; k < NC; k += NT) {
             const int r = k / TX, c = k - r * TX, i = tx0 + c, j = ty0 + r;
             if (i >= n || j >= n) continue;
-            float res[4];
+            float dres[4];  // dt L
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const float *fx = FX + q * TY * (TX + 1) + r * (TX + 1) + c;
                 const float *fy = FY + q * (TY + 1) * TX + r * TX + c;
-                res[q] = -(fx[1] - fx[0]) * inv_h - (fy[TX] - fy[0]) * inv_h;
+                dres[q] = -((fx[1] - fx[0]) + (fy[TX] - fy[0])) * dt_h;
             }
             if (a.stage == 1) {
-                float d[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) d[q] = dt * res[q];
-                put_cell<float>(gd, (float *)gd.k1, j, i, d);
+                put_cell<float>(gd, (float *)gd.k1, j, i, dres);
             } else if (a.stage == 2) {
                 float d[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const float d1 = ((const float *)gd.k1)[gidx(gd, q, j, i)];
-                    d[q] = 0.25f * (d1 + dt * res[q]);
+                    d[q] = 0.25f * (d1 + dres[q]);
                 }
                 put_cell<float>(gd, (float *)gd.k2, j, i, d);
             } else {
@@ -273,7 +270,7 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const long long e = gidx(gd, q, j, i);
-                    const float d = (2.0f / 3.0f) * (((const float *)gd.k2)[e] + dt * res[q]);
+                    const float d = (2.0f / 3.0f) * (((const float *)gd.k2)[e] + dres[q]);
                     vh[q] = ((const float *)gd.st[cur])[e];
                     vl[q] = ((const float *)gd.lo[cur])[e];
                     df_add(vh[q], vl[q], d);
@@ -293,7 +290,7 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
                 put_cell2<float>(gd, (float *)gd.st[nxt], (float *)gd.lo[nxt], j, i, vh, vl);
                 float cs2 = gam * w[3] * frcp(w[0]);
                 float lam = fabsf(w[1]) + fabsf(w[2]) + fsqrt(cs2 > 1e-14f ? cs2 : 1e-14f);
-                lmax = fmax(lmax, (double)lam);
+                lmax = fmaxf(lmax, lam);  // (NaN skipped; exact in FP64 below)
             }
         }
 
@@ -305,11 +302,11 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
                 // tiles of one CTA belong to different grids: one atomic per
                 // warp and tile
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-                if ((tid & 31) == 0 && lmax > 0.0)
-                    atomicMax(&gd.ctrl->lam_acc, (unsigned long long)__double_as_longlong(lmax));
+                for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+                if ((tid & 31) == 0 && lmax > 0.0f)
+                    atomicMax(&gd.ctrl->lam_acc, (unsigned long long)__double_as_longlong((double)lmax));
             } else {
-                lacc = fmax(lacc, lmax);
+                lacc = fmax(lacc, (double)lmax);
             }
         }
         // ---- 6. next tile's halo box: wait, then release W / FX / FY --------
