@@ -49,8 +49,11 @@ def parse():
     p.add_argument("--no-forms", action="store_true", help="skip the extra FP32c measurement")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--mode", default="plain", choices=["plain", "batched", "serve", "large"],
-                   help="plain: the headline line; batched / serve / large: the other configurations")
+    p.add_argument("--mode", default="plain", choices=["plain", "batched", "serve", "large", "families"],
+                   help="plain: the headline line; batched / serve / large: the other configurations; "
+                        "families: the other flux families on their own cases")
+    p.add_argument("--families", default="up_ducros_hll,up_ducros_roe,keep,rec3,up_hllc_d2av",
+                   help="families: which ones")
     p.add_argument("--instances", type=int, default=512, help="batched: number of grids")
     p.add_argument("--plain-sample", type=int, default=32, help="batched: grids timed on the plain FP64 path")
     p.add_argument("--requests", type=int, default=48, help="serve: requests in the stream")
@@ -62,7 +65,7 @@ def parse():
     if a.n is None:
         a.n = 8192 if large else 2048
     if a.steps is None:
-        a.steps = 2000 if large else 400
+        a.steps = 2000 if large else 50 if a.mode == "families" else 400
     return a
 
 
@@ -526,6 +529,56 @@ def run_large(args):
     print(json.dumps(line), flush=True)
 
 
+# flux family -> (solver options, initial state, its case options): each on
+# the case its reference solver runs
+FAMILY_CASES = {
+    "up_ducros_hll": ({"order": 7, "bc": "periodic", "cfl": 0.5}, "kh", {}),
+    "up_ducros_roe": ({"order": 7, "bc": "periodic", "cfl": 0.5}, "kh", {}),
+    "keep": ({"bc": "periodic", "cfl": 0.4}, "keep_sod", {}),
+    "rec3": ({"bc": "periodic", "cfl": 0.4}, "rec3_sod", {}),
+    "up_hllc_d2av": ({"order": 5, "bc": "reflect", "cfl": 0.4}, "sod", {"rho_in": 10.0}),
+}
+
+
+def run_families(args):
+    """The other flux families, FP64, one grid each: cell-stage updates/s
+    over `steps` steps after `warmup`, CUDA events on the solver's stream."""
+    import torch
+
+    import fvstuff_b200 as F
+    n, K = args.n, args.steps
+    out = {}
+    for fam in args.families.split(","):
+        opts, case, cparams = FAMILY_CASES[fam]
+        stream = torch.cuda.Stream()
+        s = F.Solver(n, flux=fam, stream=stream.cuda_stream, **opts)
+        s.init_case(case, **cparams)
+        s.step(max(3, args.warmup))
+        k0 = s.sync().steps
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clk:
+            e0.record(stream)
+            s.step(K)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = s.sync()
+        done = st.steps - k0
+        out[fam] = {"value": 3.0 * n * n * done / (ms / 1e3) if done else None,
+                    "ms_per_step": ms / max(done, 1), "steps": done, "case": case, "options": opts,
+                    "status": st.status,
+                    "clocks": clk.summary()}
+        s.close()
+    line = {"metric": METRIC, "value": None, "unit": "cell-stage updates/s", "n_gpus": 1, "steps": K,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "mode": "families",
+            "config": {"workload": "each flux family on its reference solver's case, %dx%d, %d steps" % (n, n, K)},
+            "families": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -536,6 +589,8 @@ def main():
         run_serve(args)
     elif args.mode == "large":
         run_large(args)
+    elif args.mode == "families":
+        run_families(args)
     else:
         run_gpu(args)
 
