@@ -534,7 +534,9 @@ def run_large(args):
 FAMILY_CASES = {
     "up_ducros_hll": ({"order": 7, "bc": "periodic", "cfl": 0.5}, "kh", {}),
     "up_ducros_roe": ({"order": 7, "bc": "periodic", "cfl": 0.5}, "kh", {}),
-    "keep": ({"bc": "periodic", "cfl": 0.4}, "keep_sod", {}),
+    # keep_fv's low-Mach vortex (its Sod breaks down within ~25 steps in the
+    # reference scheme itself at these sizes: dt underflow)
+    "keep": ({"bc": "periodic", "cfl": 0.4}, "lmv", {}),
     "rec3": ({"bc": "periodic", "cfl": 0.4}, "rec3_sod", {}),
     "up_hllc_d2av": ({"order": 5, "bc": "reflect", "cfl": 0.4}, "sod", {"rho_in": 10.0}),
 }
