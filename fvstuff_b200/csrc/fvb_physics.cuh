@@ -219,6 +219,30 @@ __device__ __forceinline__ double fsqrt(double x)
 __device__ __forceinline__ float frcp(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ float fsqrt(float x) { return x * rsqrtf(x); }
 
+// FP64 sound speed c = sqrt(max(gp / r, 1e-14)) from gp = gamma p and the
+// density, as gp / sqrt(gp r) = gp * rsqrt(gp r): the reciprocal root (seed
+// and the third-order step of fsqrt) replaces a reciprocal of r and a
+// square root; within 2 ulp of the correctly rounded sqrt(gp / r).  The
+// floor test gp > 1e-14 r is cs2 > 1e-14 without the division (r > 0).
+// sqrt(gp / r) without the floor (gp, r >= 1e-14)
+__device__ __forceinline__ double snd_rsq_raw(double gp, double r)
+{
+#if FVB_EXACT_RCP_SQRT
+    return sqrt(gp / r);
+#else
+    const double x = gp * r;
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double e = fma(-(x * y), y, 1.0);
+    y = fma(y, e * fma(e, 0.375, 0.5), y);
+    return gp * y;
+#endif
+}
+__device__ __forceinline__ double snd_rsq(double gp, double r)
+{
+    return gp > 1e-14 * r ? snd_rsq_raw(gp, r) : 1e-7;
+}
+
 template <class R> struct GasF {
     R gam, igm1, gm1;  // gamma, 1/(gamma-1), gamma-1
 };
@@ -250,8 +274,12 @@ __device__ __forceinline__ void upface_fast(const R *s, R &vL, R &vR)
 template <class R>
 __device__ __forceinline__ void cell_ce(R r, R a, R b, R p, const GasF<R> &gs, R &c, R &E)
 {
-    R cs2 = gs.gam * p * frcp(r);
-    c = fsqrt(cs2 > FVB_LIT(R, 1e-14) ? cs2 : FVB_LIT(R, 1e-14));
+    if constexpr (sizeof(R) == 8) {
+        c = snd_rsq(gs.gam * p, r);
+    } else {
+        R cs2 = gs.gam * p * frcp(r);
+        c = fsqrt(cs2 > FVB_LIT(R, 1e-14) ? cs2 : FVB_LIT(R, 1e-14));
+    }
     E = p * gs.igm1 + R(0.5) * r * (a * a + b * b);
 }
 
@@ -346,20 +374,16 @@ __device__ __forceinline__ void face_flux_fast(const R L[4], const R Rv[4], cons
     } else {
         const R rL = L[0], uL = L[1], tL = L[2], pL = L[3];
         const R rR = Rv[0], uR = Rv[1], tR = Rv[2], pR = Rv[3];
-        R irL, irR;
+        R cL, cR;
         if constexpr (sizeof(R) == 8) {
-            // one FP64 reciprocal for both densities (rho >= 1e-14, so the
-            // product stays normal)
-            const R ip = frcp(rL * rR);
-            irL = rR * ip;
-            irR = rL * ip;
+            // no reciprocal of the densities: c = gamma p rsqrt(gamma p rho)
+            cL = snd_rsq(gs.gam * pL, rL);
+            cR = snd_rsq(gs.gam * pR, rR);
         } else {
-            irL = frcp(rL);
-            irR = frcp(rR);
+            const R cs2L = gs.gam * pL * frcp(rL), cs2R = gs.gam * pR * frcp(rR);
+            cL = fsqrt(cs2L > FVB_LIT(R, 1e-14) ? cs2L : FVB_LIT(R, 1e-14));
+            cR = fsqrt(cs2R > FVB_LIT(R, 1e-14) ? cs2R : FVB_LIT(R, 1e-14));
         }
-        R cs2L = gs.gam * pL * irL, cs2R = gs.gam * pR * irR;
-        const R cL = fsqrt(cs2L > FVB_LIT(R, 1e-14) ? cs2L : FVB_LIT(R, 1e-14));
-        const R cR = fsqrt(cs2R > FVB_LIT(R, 1e-14) ? cs2R : FVB_LIT(R, 1e-14));
         const R EL = pL * gs.igm1 + R(0.5) * rL * (uL * uL + tL * tL);
         const R ER = pR * gs.igm1 + R(0.5) * rR * (uR * uR + tR * tR);
         const R SL = dmin<R>(uL - cL, uR - cR), SR = dmax<R>(uL + cL, uR + cR);

@@ -333,8 +333,14 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
                 if (a.stage == 3) {
                     R lam;
                     if constexpr (FAST) {
-                        R cs2 = gf.gam * w[3] * frcp(w[0]);
-                        lam = dabs<R>(w[1]) + dabs<R>(w[2]) + fsqrt(cs2 > FVB_LIT(R, 1e-14) ? cs2 : FVB_LIT(R, 1e-14));
+                        R c;
+                        if constexpr (sizeof(R) == 8) {
+                            c = snd_rsq(gf.gam * w[3], w[0]);
+                        } else {
+                            R cs2 = gf.gam * w[3] * frcp(w[0]);
+                            c = fsqrt(cs2 > FVB_LIT(R, 1e-14) ? cs2 : FVB_LIT(R, 1e-14));
+                        }
+                        lam = dabs<R>(w[1]) + dabs<R>(w[2]) + c;
                     } else {
                         lam = dabs<R>(w[1]) + dabs<R>(w[2]) + sound<R>(w[3], w[0], gs);
                     }
