@@ -11,8 +11,11 @@
 // keep_ed_kernel (per-cell entropy distance, block max, atomicMax into the
 // step control) and keep_stage_kernel (tile in shared memory, every face
 // once, divergence, RK combination with floors, stores with ghost images,
-// and in stage 3 the wave-speed max for the next dt).  The step control is
-// the same device-side Ctrl as the UP path.
+// and in stage 3 the wave-speed max for the next dt).  Both convert each
+// cell of a tile once -- floored primitives, entropy and entropy variables
+// -- and form every face's terms from those, so no face repeats the
+// divisions and logarithms of its two cells.  The step control is the same
+// device-side Ctrl as the UP path.
 #include "fvb_aux.h"
 #include "fvb_physics.cuh"
 #include "fvb_device.cuh"
@@ -48,20 +51,13 @@ __device__ __forceinline__ void k_evars(const double W[4], double s, double gam,
     V[3] = -rho / p;
 }
 
-// |(U_n - U_c) . (V_n - V_c)|                        keep_fv:249-258
-__device__ __forceinline__ double k_edist(const double Wc[4], const double Uc[4], double sc, const double Wn[4],
-                                          const double Un[4], double sn, double gam)
-{
-    double Vc[4], Vn[4], ed = 0.;
-    k_evars(Wc, sc, gam, Vc);
-    k_evars(Wn, sn, gam, Vn);
-    for (int q = 0; q < 4; ++q) ed += (Un[q] - Uc[q]) * (Vn[q] - Vc[q]);
-    return fabs(ed);
-}
-
 // ECKEP central flux (Cartesian) and MOVERS-RH coefficient  keep_fv:145-219
-__device__ __forceinline__ void k_flux(const double WL[4], const double WR[4], double sL, double sR, double nx,
-                                       double ny, double gam, double Fec[4], double *alphaS)
+// VL, VR: the two cells' entropy variables in the face frame (the Cartesian
+// ones of k_evars with (u, v) -> (un, ut): for the normals (1, 0) and (0, 1)
+// a relabelling and one exact negation, so the values are the reference's)
+__device__ __forceinline__ void k_flux(const double WL[4], const double WR[4], const double VL[4],
+                                       const double VR[4], double nx, double ny, double gam, double Fec[4],
+                                       double *alphaS)
 {
     const double rL = WL[0], uL = WL[1], vL = WL[2], pL = WL[3];
     const double rR = WR[0], uR = WR[1], vR = WR[2], pR = WR[3];
@@ -73,10 +69,6 @@ __device__ __forceinline__ void k_flux(const double WL[4], const double WR[4], d
     const double UR[4] = {rR, rR * unR, rR * utR, ER};
     const double FL[4] = {rL * unL, rL * unL * unL + pL, rL * unL * utL, (EL + pL) * unL};
     const double FR[4] = {rR * unR, rR * unR * unR + pR, rR * unR * utR, (ER + pR) * unR};
-    const double VL[4] = {(gam - sL) / (gam - 1.) - rL * (unL * unL + utL * utL) / (2. * pL), rL * unL / pL,
-                          rL * utL / pL, -rL / pL};
-    const double VR[4] = {(gam - sR) / (gam - 1.) - rR * (unR * unR + utR * utR) / (2. * pR), rR * unR / pR,
-                          rR * utR / pR, -rR / pR};
     const double dV0 = VR[0] - VL[0], dV1 = VR[1] - VL[1], dV2 = VR[2] - VL[2], dV3 = VR[3] - VL[3];
     const double dpsi = rR * unR - rL * unL;
     const double Fc0 = 0.5 * (FL[0] + FR[0]);
@@ -117,37 +109,6 @@ __device__ __forceinline__ void load_cell(const double *buf, const GridDev &gd, 
     for (int q = 0; q < 4; ++q) U[q] = buf[e + q * gd.plane];
 }
 
-// per-cell max of the entropy distance across its right and top faces,
-// max-reduced into ctrl->aux                       keep_fv_euler_2d.cu:260-277
-__global__ void keep_ed_kernel(const GridDev gd, const double *buf)
-{
-    __shared__ double sh[32];
-    const int n = gd.n;
-    const long long n2 = (long long)n * n;
-    double m = 0.0;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
-         k += (long long)blockDim.x * gridDim.x) {
-        const int j = (int)(k / n), i = (int)(k % n);
-        double Uc[4], Ux[4], Uy[4], Wc[4], Wx[4], Wy[4], Fc[4], Fx[4], Fy[4], sc, sx, sy;
-        load_cell(buf, gd, j, i, Uc);
-        load_cell(buf, gd, j, i + 1, Ux);
-        load_cell(buf, gd, j + 1, i, Uy);
-        k_cell(Uc, gd.gam, Wc, Fc, sc);
-        k_cell(Ux, gd.gam, Wx, Fx, sx);
-        k_cell(Uy, gd.gam, Wy, Fy, sy);
-        double ed = fmax(k_edist(Wc, Fc, sc, Wx, Fx, sx, gd.gam), k_edist(Wc, Fc, sc, Wy, Fy, sy, gd.gam));
-        m = fmax(m, ed);
-    }
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double b = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, sh[w]);
-        atomicMax(&gd.ctrl->aux, (unsigned long long)__double_as_longlong(b));
-    }
-}
-
 struct KCtl {
     double dt;
     int run;
@@ -155,6 +116,55 @@ struct KCtl {
 
 constexpr int KTX = 32, KTY = 16, KNT = 256, KG = 2;
 constexpr int KSW = KTX + 2 * KG, KSH = KTY + 2 * KG, KPL = KSW * KSH;
+constexpr int EW = KTX + 1, EH = KTY + 1, EPL = EW * EH;  // a tile and its right / top neighbours
+
+// per-cell max of the entropy distance |(U_n - U_c) . (V_n - V_c)| across
+// its right and top faces, max-reduced into ctrl->aux; a tile's cells and
+// their right / top neighbours are converted once each (floored conserved
+// state and entropy variables in shared memory)   keep_fv_euler_2d.cu:249-277
+__global__ void __launch_bounds__(KNT) keep_ed_kernel(const GridDev gd, const double *buf, int ntiles)
+{
+    __shared__ double sU[4][EPL], sV[4][EPL];
+    __shared__ double sh[KNT / 32];
+    const int tid = threadIdx.x, n = gd.n;
+    double m = 0.0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int tx0 = (t % gd.tiles_x) * KTX, ty0 = (t / gd.tiles_x) * KTY;
+        for (int k = tid; k < EPL; k += KNT) {
+            const int r = k / EW, c = k - r * EW, j = ty0 + r, i = tx0 + c;
+            double U[4] = {1, 0, 0, 2.5};  // admissible filler beyond the ghost layer
+            if (j <= n && i <= n) load_cell(buf, gd, j, i, U);
+            double W[4], Uf[4], sc, V[4];
+            k_cell(U, gd.gam, W, Uf, sc);
+            k_evars(W, sc, gd.gam, V);
+            for (int q = 0; q < 4; ++q) {
+                sU[q][k] = Uf[q];
+                sV[q][k] = V[q];
+            }
+        }
+        __syncthreads();
+        for (int k = tid; k < KTX * KTY; k += KNT) {
+            const int r = k / KTX, c = k - r * KTX;
+            if (ty0 + r >= n || tx0 + c >= n) continue;
+            const int b = r * EW + c;
+            double ex = 0., ey = 0.;
+            for (int q = 0; q < 4; ++q) {
+                ex += (sU[q][b + 1] - sU[q][b]) * (sV[q][b + 1] - sV[q][b]);
+                ey += (sU[q][b + EW] - sU[q][b]) * (sV[q][b + EW] - sV[q][b]);
+            }
+            m = fmax(m, fmax(fabs(ex), fabs(ey)));
+        }
+        __syncthreads();
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((tid & 31) == 0) sh[tid >> 5] = m;
+    __syncthreads();
+    if (tid == 0) {
+        double b = 0.0;
+        for (int w = 0; w < KNT / 32; ++w) b = fmax(b, sh[w]);
+        atomicMax(&gd.ctrl->aux, (unsigned long long)__double_as_longlong(b));
+    }
+}
 
 // one SSP-RK3 stage of the KEEP scheme               keep_fv_euler_2d.cu:298-393
 __global__ void __launch_bounds__(KNT, 2) keep_stage_kernel(const GridDev gd, int stage, int ntiles)
@@ -163,7 +173,8 @@ __global__ void __launch_bounds__(KNT, 2) keep_stage_kernel(const GridDev gd, in
     double *U = reinterpret_cast<double *>(smem_raw);  // [4][KSH][KSW] conserved, rho floored
     double *W = U + 4 * KPL;                           // [4] floored primitives
     double *S = W + 4 * KPL;                           // entropy
-    double *FX = S + KPL;                              // [4][KTY][KTX+1]
+    double *V = S + KPL;                               // [4] entropy variables (Cartesian)
+    double *FX = V + 4 * KPL;                          // [4][KTY][KTX+1]
     double *FY = FX + 4 * KTY * (KTX + 1);             // [4][KTY+1][KTX]
     __shared__ KCtl s_ctl;
     __shared__ double s_red[KNT / 32];
@@ -194,11 +205,13 @@ __global__ void __launch_bounds__(KNT, 2) keep_stage_kernel(const GridDev gd, in
                 long long e = (long long)jp * gd.pitch + ip + gd.xoff;
                 for (int q = 0; q < 4; ++q) Uc[q] = in[e + q * gd.plane];
             }
-            double Wc[4], Fc[4], sc;
+            double Wc[4], Fc[4], sc, Vc[4];
             k_cell(Uc, gam, Wc, Fc, sc);
+            k_evars(Wc, sc, gam, Vc);
             for (int q = 0; q < 4; ++q) {
                 U[q * KPL + k] = Fc[q];
                 W[q * KPL + k] = Wc[q];
+                V[q * KPL + k] = Vc[q];
             }
             S[k] = sc;
         }
@@ -212,19 +225,25 @@ __global__ void __launch_bounds__(KNT, 2) keep_stage_kernel(const GridDev gd, in
             else { const int f2 = f - (KTX + 1) * KTY; r = f2 / KTX; c = f2 - r * KTX; st = KSW; }
             const int b = (r + KG) * KSW + (c + KG), a = b - st;
             const double nx = xf ? 1. : 0., ny = xf ? 0. : 1.;
-            double WL[4], WR[4], UL[4], UR[4], Up2[4], Um1[4], fec[4], aS;
+            double WL[4], WR[4], UL[4], UR[4], Up2[4], Um1[4], VL[4], VR[4], fec[4], aS;
             for (int q = 0; q < 4; ++q) {
                 WL[q] = W[q * KPL + a]; WR[q] = W[q * KPL + b];
                 UL[q] = U[q * KPL + a]; UR[q] = U[q * KPL + b];
                 Up2[q] = U[q * KPL + b + st]; Um1[q] = U[q * KPL + a - st];
+                VL[q] = V[q * KPL + a]; VR[q] = V[q * KPL + b];
             }
-            const double sL = S[a], sR = S[b];
-            k_flux(WL, WR, sL, sR, nx, ny, gam, fec, &aS);
+            // face frame: (un, ut) = (u, v) on x-faces, (v, -u) on y-faces
+            const double VLn[4] = {VL[0], xf ? VL[1] : VL[2], xf ? VL[2] : -VL[1], VL[3]};
+            const double VRn[4] = {VR[0], xf ? VR[1] : VR[2], xf ? VR[2] : -VR[1], VR[3]};
+            k_flux(WL, WR, VLn, VRn, nx, ny, gam, fec, &aS);
             const double unL = WL[1] * nx + WL[2] * ny, unR = WR[1] * nx + WR[2] * ny;
             const double aR = k_snd(0.5 * (WL[0] + WR[0]), 0.5 * (WL[3] + WR[3]), gam);
             const double lamt = fmax(fabs(unL), fabs(unR)) + aR;
             const double aJST = (1.0 / 32.0) * lamt;
-            const double sed = k_edist(WL, UL, sL, WR, UR, sR, gam) / (edmax + 1e-30);
+            // entropy distance of the face                  keep_fv:249-258
+            double ed = 0.;
+            for (int q = 0; q < 4; ++q) ed += (UR[q] - UL[q]) * (VR[q] - VL[q]);
+            const double sed = fabs(ed) / (edmax + 1e-30);
             const double phi = (1. - exp(-12.0 * sed)) > 0.05 ? 1. : 0.;
             double *o = xf ? FX + r * (KTX + 1) + c : FY + r * KTX + c;
             const int os = xf ? KTY * (KTX + 1) : (KTY + 1) * KTX;
@@ -301,7 +320,7 @@ __global__ void keep_lam_kernel(const GridDev gd)
     }
 }
 
-size_t keep_smem() { return sizeof(double) * (9 * KPL + 4 * KTY * (KTX + 1) + 4 * (KTY + 1) * KTX); }
+size_t keep_smem() { return sizeof(double) * (13 * KPL + 4 * KTY * (KTX + 1) + 4 * (KTY + 1) * KTX); }
 
 }  // namespace
 
@@ -331,9 +350,8 @@ cudaError_t keep_launch_stage(const GridDev &gd, int stage, int tiles, cudaStrea
     const void *in = stage == 2 ? gd.k1 : stage == 3 ? gd.k2 : gd.st[0];
     cudaError_t e = cudaMemsetAsync(&gd.ctrl->aux, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
-    int eb = (int)(((long long)gd.n * gd.n + 255) / 256);
-    if (eb > 4 * sms) eb = 4 * sms;
-    keep_ed_kernel<<<eb, 256, 0, s>>>(gd, (const double *)in);
+    const int eb = tiles < 4 * sms ? tiles : 4 * sms;
+    keep_ed_kernel<<<eb, KNT, 0, s>>>(gd, (const double *)in, tiles);
     const int grid = tiles < ctas_per_sm * sms ? tiles : ctas_per_sm * sms;
     keep_stage_kernel<<<grid, KNT, keep_smem(), s>>>(gd, stage, tiles);
     return cudaGetLastError();

@@ -298,9 +298,8 @@ __device__ __forceinline__ void hll_fast(const R L[4], const R Rv[4], const GasF
     const R zero = R(0);
     const R rL = L[0], uL = L[1], tL = L[2], pL = L[3];
     const R rR = Rv[0], uR = Rv[1], tR = Rv[2], pR = Rv[3];
-    const R ip = frcp(rL * rR);
     // sound speed without a floor, as carb_fv_2d.cu:60-61 (rho, p >= 1e-14)
-    const R cL = fsqrt(gs.gam * pL * (rR * ip)), cR = fsqrt(gs.gam * pR * (rL * ip));
+    const R cL = snd_rsq_raw(gs.gam * pL, rL), cR = snd_rsq_raw(gs.gam * pR, rR);
     const R EL = pL * gs.igm1 + R(0.5) * rL * (uL * uL + tL * tL);
     const R ER = pR * gs.igm1 + R(0.5) * rR * (uR * uR + tR * tR);
     // Einfeldt's form of the two-wave average: FL, FR or the subsonic
