@@ -81,15 +81,22 @@ __device__ void r3_hllc(const double L[4], const double R[4], double F[4])
 }
 
 // Zhang-Shu scaling of a face state toward its cell average (linear for
-// rho, 25-step bisection for p)                fv_rec3_2d.cu:125-145
-__device__ void r3_scale(const double Ub[4], double U[4])
+// rho, 25-step bisection for p), then its floored primitives: the density,
+// velocity and pressure that the pressure test forms are the primitives'
+// own unless the bisection moved the state, so they are reused (the same
+// operations on the same values as scaling, then converting)
+//                                               fv_rec3_2d.cu:125-145, :71-79
+__device__ __forceinline__ void r3_scale_w(const double Ub[4], double U[4], double W[4])
 {
     if (U[0] < R3_RHOFLOOR) {
         const double d = Ub[0] - U[0];
         const double th = (d > 0.) ? (Ub[0] - R3_RHOFLOOR) / d : 0.;
         for (int q = 0; q < 4; q++) U[q] = Ub[q] + th * (U[q] - Ub[q]);
     }
-    if (r3_p(U) < R3_PFLOOR) {
+    double r = fmax(U[0], R3_RHOFLOOR);
+    double u = U[1] / r, v = U[2] / r;
+    double p = (R3_GAM - 1.0) * (U[3] - 0.5 * r * (u * u + v * v));
+    if (p < R3_PFLOOR) {
         double lo = 0., hi = 1.;
         for (int it = 0; it < 25; it++) {
             const double mid = 0.5 * (lo + hi);
@@ -99,7 +106,12 @@ __device__ void r3_scale(const double Ub[4], double U[4])
             else hi = mid;
         }
         for (int q = 0; q < 4; q++) U[q] = Ub[q] + lo * (U[q] - Ub[q]);
+        r = fmax(U[0], R3_RHOFLOOR);
+        u = U[1] / r;
+        v = U[2] / r;
+        p = (R3_GAM - 1.0) * (U[3] - 0.5 * r * (u * u + v * v));
     }
+    W[0] = r; W[1] = u; W[2] = v; W[3] = fmax(p, R3_PFLOOR);
 }
 
 // 2x2-block limiter on U[c][q] (cells c = 0..3: (i0,j0), (i0+1,j0),
@@ -217,11 +229,9 @@ __global__ void __launch_bounds__(RNT, 2) rec3_stage_kernel(const GridDev gd, in
                 UbL[q] = uc;
                 UbR[q] = up;
             }
-            r3_scale(UbL, UL);
-            r3_scale(UbR, UR);
             double WL[4], WR[4], L[4], Rr[4], Fn[4];
-            r3_w(UL, WL);
-            r3_w(UR, WR);
+            r3_scale_w(UbL, UL, WL);
+            r3_scale_w(UbR, UR, WR);
             const int QN = xf ? 1 : 2, QT = xf ? 2 : 1;
             L[0] = WL[0]; L[1] = WL[QN]; L[2] = WL[QT]; L[3] = WL[3];
             Rr[0] = WR[0]; Rr[1] = WR[QN]; Rr[2] = WR[QT]; Rr[3] = WR[3];

@@ -502,3 +502,20 @@ def refg_bak_run(U: np.ndarray, N: int, h: float, cfl: float, max_steps: int, t_
     if st > 0:
         raise RuntimeError("reference GPU run failed: cuda error %d" % st)
     return -int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3]), float(ms.value)
+
+
+def have_ref_gpu_rec3() -> bool:
+    return (REF / "libref_gpu_rec3.so").exists()
+
+
+def refg_rec3_run(U: np.ndarray, N: int, h: float, cfl: float, max_steps: int, t_stop: float = 1e30):
+    """fv_rec3_2d.cu's kernels and loop on the GPU (FP64; padded U after its
+    limiter pass and ghost fill, in place); (status, t, steps, lam_max,
+    last_dt, ms of the stepping loop)."""
+    info = np.zeros(4)
+    ms = C.c_float(0)
+    st = ref_gpu("rec3").refg_rec3_run(_ptr(U), C.c_int(N), C.c_double(h), C.c_double(cfl), C.c_int(max_steps),
+                                       C.c_double(t_stop), _ptr(info), C.byref(ms))
+    if st > 0:
+        raise RuntimeError("reference GPU run failed: cuda error %d" % st)
+    return -int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3]), float(ms.value)

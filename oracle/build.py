@@ -169,6 +169,9 @@ def build_ref(verbose: bool = False, gpu: bool = True) -> list[Path]:
         ]
         if bak.exists():
             dev.append(("libref_gpu_bak.so", ["-DREF_BAK", '-DREF_CU="%s"' % bak], bak))
+        if rec3.exists():
+            dev.append(("libref_gpu_rec3.so", ["-DREF_REC3", "-Dreal=double", "-Dreall=double",
+                                               '-DREF_CU="%s"' % rec3], rec3))
         for name, defs, src in dev:
             out = OUT / name
             if _stale(out, [src, HERE / "ref_gpu.cu", HERE / "build.py"]):

@@ -280,4 +280,73 @@ int refg_bak_run(R *Uh, int N, R h, R cfl, R C2, R Cg, R sc, int order, int max_
 }
 
 }  /* extern "C" */
+
+#elif defined(REF_REC3)
+/* fv_rec3_2d.cu built with real = reall = double */
+typedef double R;
+
+extern "C" {
+
+/* the time loop of fv_rec3_2d.cu:551-590 with its kernels and launches
+ * (memset + atomicAdd-scatter compute_rhs, rk_stage, the 2x2-block limiter,
+ * apply_bc, gpu_max) on a padded conserved state that has had its limiter
+ * pass and ghost fill; ms_out: CUDA-event time of the stepping loop */
+int refg_rec3_run(R *Uh, int N, R h, R cfl, int max_steps, double t_stop, double *info, float *ms_out)
+{
+    int Np = N + 2 * G_GHOST;
+    size_t szP = (size_t)NVAR * Np * Np * sizeof(R), szC = (size_t)NVAR * N * N * sizeof(R);
+    R *dU, *dU0, *dU1, *dRHS, *dlam, *dtmp;
+    RET_ON_ERR(cudaMalloc(&dU, szP)); RET_ON_ERR(cudaMalloc(&dU0, szP)); RET_ON_ERR(cudaMalloc(&dU1, szP));
+    RET_ON_ERR(cudaMalloc(&dRHS, szC));
+    RET_ON_ERR(cudaMalloc(&dlam, (size_t)N * N * sizeof(R)));
+    RET_ON_ERR(cudaMalloc(&dtmp, 65 * sizeof(R)));
+    RET_ON_ERR(cudaMemcpy(dU, Uh, szP, cudaMemcpyHostToDevice));
+    RET_ON_ERR(cudaMemset(dRHS, 0, szC));
+    compute_rhs<<<GS_NBLK, BLOCK1D>>>(dU, dRHS, dlam, N, Np, h);
+    RET_ON_ERR(cudaDeviceSynchronize());
+    R lmax = gpu_max(dlam, dtmp, N * N), t = 0, dt = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    int step = 0, status = 0;
+    while (step < max_steps && t < t_stop) {
+        if (!(lmax > 0.)) { status = 1; break; }
+        dt = cfl * h / lmax;
+        if (t + dt > t_stop) dt = t_stop - t;
+        if (dt < 1e-14) { status = 2; break; }
+        RET_ON_ERR(cudaMemcpy(dU0, dU, szP, cudaMemcpyDeviceToDevice));
+        rk_stage<<<GS_NBLK, BLOCK1D>>>(dU1, dU0, dU0, dRHS, 0., 1., 0., dt, N, Np);
+        limit_positivity_blocks<<<GS_NBLK, BLOCK1D>>>(dU1, N, Np);
+        apply_bc<<<GS_NBLK, BLOCK1D>>>(dU1, N, Np);
+        RET_ON_ERR(cudaMemset(dRHS, 0, szC));
+        compute_rhs<<<GS_NBLK, BLOCK1D>>>(dU1, dRHS, dlam, N, Np, h);
+        rk_stage<<<GS_NBLK, BLOCK1D>>>(dU1, dU0, dU1, dRHS, 0.75, 0.25, 0., dt, N, Np);
+        limit_positivity_blocks<<<GS_NBLK, BLOCK1D>>>(dU1, N, Np);
+        apply_bc<<<GS_NBLK, BLOCK1D>>>(dU1, N, Np);
+        RET_ON_ERR(cudaMemset(dRHS, 0, szC));
+        compute_rhs<<<GS_NBLK, BLOCK1D>>>(dU1, dRHS, dlam, N, Np, h);
+        rk_stage<<<GS_NBLK, BLOCK1D>>>(dU, dU0, dU1, dRHS, (R)(1. / 3.), (R)(2. / 3.), 0., dt, N, Np);
+        limit_positivity_blocks<<<GS_NBLK, BLOCK1D>>>(dU, N, Np);
+        apply_bc<<<GS_NBLK, BLOCK1D>>>(dU, N, Np);
+        RET_ON_ERR(cudaMemset(dRHS, 0, szC));
+        compute_rhs<<<GS_NBLK, BLOCK1D>>>(dU, dRHS, dlam, N, Np, h);
+        RET_ON_ERR(cudaDeviceSynchronize());
+        lmax = gpu_max(dlam, dtmp, N * N);
+        t += dt;
+        step++;
+    }
+    cudaEventRecord(e1);
+    RET_ON_ERR(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms_out) *ms_out = ms;
+    RET_ON_ERR(cudaGetLastError());
+    RET_ON_ERR(cudaMemcpy(Uh, dU, szP, cudaMemcpyDeviceToHost));
+    if (info) { info[0] = t; info[1] = step; info[2] = lmax; info[3] = dt; }
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    cudaFree(dU); cudaFree(dU0); cudaFree(dU1); cudaFree(dRHS); cudaFree(dlam); cudaFree(dtmp);
+    return status ? -status : 0;
+}
+
+}  /* extern "C" */
 #endif
