@@ -7,7 +7,7 @@
 // 6th-order divergence of the velocity (compressions only).  SSP-RK3 on
 // conserved variables, no floors; FP64.
 //
-// One launch per stage does all of it for a tile of 32 x 16 cells: the halo
+// One launch per stage does all of it for a tile of 32 x 8 cells: the halo
 // box of the stage input (g = max((order+1)/2, 3) layers, the sensor's reach)
 // goes to shared memory together with each box cell's sensor velocities,
 // |u|+c, |v|+c and c; every face flux is computed once; each cell then
@@ -26,7 +26,7 @@
 namespace fvb {
 namespace {
 
-constexpr int DTX = 32, DTY = 16, DNT = 256;
+constexpr int DTX = 32, DTY = 8, DNT = 256;
 
 // conserved -> p, c, u, v; no density floor, c^2 floored at 1e-14
 //                                          fv_up7_ducros_2d.cu.bak:65-74
@@ -101,11 +101,15 @@ struct D2Shape {
     static constexpr int NFX = (DTX + 1) * DTY, NFY = DTX * (DTY + 1);
     // Q[4][PL] | SU, SV, LX, LY, CS [PL each] | FX[4][NFX] | FY[4][NFY]
     static constexpr size_t SMEM = sizeof(double) * (9 * PL + 4 * NFX + 4 * NFY);
+    // resident CTAs an SM is compiled for: four (56 KB each, <= 64
+    // registers) with the 3-cell halo, three (64 KB) with UP7's 4
+    static constexpr int MINB = HB == 3 ? 4 : 3;
 };
 
 // one SSP-RK3 stage                        fv_up7_ducros_2d.cu.bak:287-446
 template <int ORDER>
-__global__ void __launch_bounds__(DNT, 2) d2av_stage_kernel(const GridDev gd, int stage, int ntiles, D2Params av)
+__global__ void __launch_bounds__(DNT, D2Shape<ORDER>::MINB)
+    d2av_stage_kernel(const GridDev gd, int stage, int ntiles, D2Params av)
 {
     using S = D2Shape<ORDER>;
     constexpr int HW = S::HW, HB = S::HB, BW = S::BW, PL = S::PL;
