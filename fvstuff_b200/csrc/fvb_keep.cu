@@ -172,8 +172,7 @@ __global__ void __launch_bounds__(KNT, 2) keep_stage_kernel(const GridDev gd, in
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *U = reinterpret_cast<double *>(smem_raw);  // [4][KSH][KSW] conserved, rho floored
     double *W = U + 4 * KPL;                           // [4] floored primitives
-    double *S = W + 4 * KPL;                           // entropy
-    double *V = S + KPL;                               // [4] entropy variables (Cartesian)
+    double *V = W + 4 * KPL;                           // [4] entropy variables (Cartesian)
     double *FX = V + 4 * KPL;                          // [4][KTY][KTX+1]
     double *FY = FX + 4 * KTY * (KTX + 1);             // [4][KTY+1][KTX]
     __shared__ KCtl s_ctl;
@@ -213,7 +212,6 @@ __global__ void __launch_bounds__(KNT, 2) keep_stage_kernel(const GridDev gd, in
                 W[q * KPL + k] = Wc[q];
                 V[q * KPL + k] = Vc[q];
             }
-            S[k] = sc;
         }
         __syncthreads();
         // faces: x then y; the face lies between cells a (left/bottom) and
@@ -320,7 +318,7 @@ __global__ void keep_lam_kernel(const GridDev gd)
     }
 }
 
-size_t keep_smem() { return sizeof(double) * (13 * KPL + 4 * KTY * (KTX + 1) + 4 * (KTY + 1) * KTX); }
+size_t keep_smem() { return sizeof(double) * (12 * KPL + 4 * KTY * (KTX + 1) + 4 * (KTY + 1) * KTX); }
 
 }  // namespace
 
