@@ -134,16 +134,24 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profiles(precision: str, n: int):
-    """dram bytes per stage launch from the committed ncu summary, if any."""
+def _profile_value(precision: str, n: int, key: str):
+    """A number from the committed ncu summary of the stage kernel, if any."""
     kernel = "stage32c_kernel" if precision == "f32c" else "stage_kernel"
     f = ROOT / "profiles" / ("%s_kh%d_%s.txt" % (kernel, n, precision))
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch_full_size:"):
-            return float(line.split(":", 1)[1])
+        if line.startswith(key):
+            try:
+                return float(line[len(key):].lstrip(": ").split()[0])
+            except (IndexError, ValueError):
+                return None
     return None
+
+
+def traffic_from_profiles(precision: str, n: int):
+    """dram bytes per stage launch from the committed ncu summary, if any."""
+    return _profile_value(precision, n, "traffic_bytes_per_launch_full_size:")
 
 
 # ---------------------------------------------------------------------------
@@ -276,7 +284,12 @@ def run_gpu(args):
                          "traffic": traffic_from_profiles(args.precision, n),
                          "peak_kind": peak_kind,
                          "bytes_per_cell_stage": BYTES_PER_CELL_STAGE[args.precision],
-                         "kernel": "fvb::stage_kernel (one launch per RK stage)"},
+                         "kernel": "fvb::stage_kernel (one launch per RK stage)",
+                         # what bounds it instead (ncu summary of the same kernel): the FP64
+                         # pipe, busy this share of the time; at 100 % the stage would
+                         # still move only ~45 % of the HBM peak
+                         "fp64_pipe_pct_ncu": _profile_value(args.precision, n, "pipe_fp64_pct"),
+                         "issue_active_pct_ncu": _profile_value(args.precision, n, "issue_active_pct")},
             "clocks": clk.summary()}
 
     if not args.no_forms and args.precision == "f64":
