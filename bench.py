@@ -49,9 +49,12 @@ def parse():
     p.add_argument("--no-forms", action="store_true", help="skip the extra FP32c measurement")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--mode", default="plain", choices=["plain", "batched", "serve", "large", "families"],
+    p.add_argument("--mode", default="plain",
+                   choices=["plain", "batched", "serve", "large", "families", "precision"],
                    help="plain: the headline line; batched / serve / large: the other configurations; "
-                        "families: the other flux families on their own cases")
+                        "families: the other flux families on their own cases; precision: FP32c against "
+                        "FP64 over a whole run")
+    p.add_argument("--t-end", type=float, default=1.0, help="precision: final time of the KH run")
     p.add_argument("--families", default="up_ducros_hll,up_ducros_roe,keep,rec3,up_hllc_d2av",
                    help="families: which ones")
     p.add_argument("--instances", type=int, default=512, help="batched: number of grids")
@@ -594,6 +597,68 @@ def run_families(args):
     print(json.dumps(line), flush=True)
 
 
+def _density_errors(a, b):
+    """relative L1 and L-inf of density a against b (interior arrays)"""
+    d = np.abs(a - b)
+    return float(d.sum() / np.abs(b).sum()), float(d.max() / np.abs(b).max())
+
+
+def run_precision(args):
+    """FP32c against the plain FP64 form (itself held to the oracle at 1e-12)
+    over whole runs: Kelvin-Helmholtz n^2 to t_end with the error of density
+    at every tenth of the run, and the periodic isentropic vortex 256^2 over
+    one period (t = 10).  Both forms land exactly on each checkpoint time.
+    Beside the KH curve, the same FP64 run started from a density one ulp
+    away in every cell: how far the flow itself carries a last-bit change."""
+    import torch
+
+    import fvstuff_b200 as F
+    n, t_end = args.n, args.t_end
+    curve = []
+    a = F.Solver(n, bc="periodic", cfl=0.5, precision="f64")
+    b = F.Solver(n, bc="periodic", cfl=0.5, precision="f32c")
+    c = F.Solver(n, bc="periodic", cfl=0.5, precision="f64")
+    a.init_case("kh")
+    b.init_case("kh")
+    w = a.get_state(interior=True)
+    w[0] = np.nextafter(w[0], np.inf)
+    c.set_state(w, interior=True)
+    for k in range(1, 11):
+        t = t_end * k / 10
+        sa, sb, sc = a.advance(t), b.advance(t), c.advance(t)
+        ra = a.get_state(interior=True)[0]
+        l1, linf = _density_errors(b.get_state(interior=True)[0], ra)
+        p1, pinf = _density_errors(c.get_state(interior=True)[0], ra)
+        curve.append({"t": t, "l1_rel": l1, "linf_rel": linf, "f64_1ulp_l1_rel": p1, "f64_1ulp_linf_rel": pinf,
+                      "steps_f64": sa.steps, "steps_f32c": sb.steps, "status": [sa.status, sb.status, sc.status]})
+        print("KH %d^2 t=%.2f: FP32c L1 %.3e Linf %.3e | FP64 1-ulp start L1 %.3e Linf %.3e (steps %d / %d)"
+              % (n, t, l1, linf, p1, pinf, sa.steps, sb.steps), file=sys.stderr, flush=True)
+    a.close()
+    b.close()
+    c.close()
+    sys.path.insert(0, str(ROOT / "tests"))
+    from cases import vortex
+    m = 256
+    w0 = vortex(m)
+    res = {}
+    for prec in ("f64", "f32c"):
+        s = F.Solver(m, bc="periodic", x0=-5.0, y0=-5.0, length=10.0, cfl=0.5, precision=prec)
+        s.set_state(w0, layout="prim", interior=True)
+        st = s.advance(10.0)
+        res[prec] = (s.get_state(interior=True)[0], st)
+        s.close()
+    torch.cuda.synchronize()
+    vl1, vlinf = _density_errors(res["f32c"][0], res["f64"][0])
+    line = {"metric": METRIC, "value": curve[-1]["l1_rel"], "unit": "relative L1 density error, FP32c vs FP64",
+            "n_gpus": 1, "higher_is_better": False, "dtype": "f32c", "data": "synthetic", "mode": "precision",
+            "config": {"workload": "kelvin-helmholtz %dx%d periodic CFL 0.5 to t=%g, FP32c and FP64 side by side; "
+                                   "isentropic vortex 256^2 periodic, one period" % (n, n, t_end)},
+            "kh_curve": curve,
+            "vortex_one_period": {"l1_rel": vl1, "linf_rel": vlinf, "steps_f64": res["f64"][1].steps,
+                                  "steps_f32c": res["f32c"][1].steps}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -606,6 +671,8 @@ def main():
         run_large(args)
     elif args.mode == "families":
         run_families(args)
+    elif args.mode == "precision":
+        run_precision(args)
     else:
         run_gpu(args)
 
