@@ -527,7 +527,8 @@ cudaError_t ctrl_set(Ctrl *c, double t_stop, int reset, double t0, double cfl, d
 // ---------------------------------------------------------------------------
 // frame fields of fv_up7's composite image, from an FP32 primitive IDX_P
 // array with its ghost ring: density, 6th-order vorticity (dv/dx - du/dy,
-// central differences over +-3 cells; 0 when the ghost ring is narrower),
+// central differences over +-3 cells; 4th-order over +-2 with the two ghost
+// layers of the KEEP and rec3 families),
 // the Ducros cell sensor (max over the cell's four faces of
 // dp^2 / (dp^2 + 0.1 (pa + pb)^2)), |v| and pressure.  Output: 5 planes of
 // n x n floats, row-major, j = 0 at the bottom.
@@ -557,6 +558,13 @@ __global__ void frame_kernel(const float *Q, int n, int g, int np, float h, floa
             const float dudy = -at(1, jp - 3, ip) + 9.0f * at(1, jp - 2, ip) - 45.0f * at(1, jp - 1, ip) +
                                45.0f * at(1, jp + 1, ip) - 9.0f * at(1, jp + 2, ip) + at(1, jp + 3, ip);
             w = (dvdx - dudy) / (60.0f * h);
+        } else {
+            // two ghost layers (KEEP, rec3): the 4th-order central difference
+            const float dvdx = at(2, jp, ip - 2) - 8.0f * at(2, jp, ip - 1) + 8.0f * at(2, jp, ip + 1) -
+                               at(2, jp, ip + 2);
+            const float dudy = at(1, jp - 2, ip) - 8.0f * at(1, jp - 1, ip) + 8.0f * at(1, jp + 1, ip) -
+                               at(1, jp + 2, ip);
+            w = (dvdx - dudy) / (12.0f * h);
         }
         const float u = at(1, jp, ip), v = at(2, jp, ip);
         out[k] = at(0, jp, ip);

@@ -169,8 +169,10 @@ FVB_API fvb_status fvb_get_state_hilo(fvb_solver *s, float *hi, float *lo);
 
 /* Frame fields of fv_up7's composite image (fv_up7_ducros_2d.cu:800-829,
  * :511-526), extracted on the device from the state as it stands after the
- * steps already enqueued: density, 6th-order vorticity, the Ducros cell
- * sensor, |v| and pressure, 5 planes of N x N floats (row-major, j = 0 at the
+ * steps already enqueued: density, 6th-order vorticity (4th-order for the
+ * two-ghost-layer KEEP and rec3 families), the Ducros cell sensor (for
+ * FVB_FLUX_UP_HLLC_D2AV its velocity-divergence weight), |v| and pressure,
+ * 5 planes of N x N floats (row-major, j = 0 at the
  * bottom).  fvb_frame_begin enqueues the extraction on the solver's stream and
  * the copy to host on a second stream, and returns; steps enqueued after it
  * run while the frame is copied and written.  fvb_frame_end waits for that
