@@ -185,6 +185,13 @@ class Solver:
         FVB_ERR_TIMEOUT (see fvb_debug_drop_load)."""
         check(lib().fvb_debug_drop_load(self._h), "fvb_debug_drop_load")
 
+    def limiter_fixes(self) -> int:
+        """rec3 family: blocks whose mean needed the floor fix since the
+        state was set (see fvb_limiter_fixes); 0 for the other families."""
+        v = C.c_int64(0)
+        check(lib().fvb_limiter_fixes(self._h, C.byref(v)), "fvb_limiter_fixes")
+        return int(v.value)
+
     def set_d2av(self, c2: float = 0.5, cg: float = 0.0, sc: float = 0.05) -> None:
         """Coefficients of the 'up_hllc_d2av' viscosity (the .bak solver's
         C2, Cg and sc arguments; see fvb_set_d2av)."""

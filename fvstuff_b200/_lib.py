@@ -81,6 +81,7 @@ _SIG = {
     "fvb_frame_begin": (C.c_int, [_P]),
     "fvb_debug_drop_load": (C.c_int, [_P]),
     "fvb_set_d2av": (C.c_int, [_P, C.c_double, C.c_double, C.c_double]),
+    "fvb_limiter_fixes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "fvb_frame_end": (C.c_int, [_P, _P]),
     "fvb_save": (C.c_int, [_P, C.c_char_p]),
     "fvb_load": (C.c_int, [_P, C.c_char_p]),

@@ -526,6 +526,19 @@ fvb_status fvb_get_state(fvb_solver *s, void *dst, int layout, int dtype, int wh
     return FVB_OK;
 }
 
+fvb_status fvb_limiter_fixes(fvb_solver *s, int64_t *count)
+{
+    if (!s || !count) return fail(FVB_ERR_INVALID, "null argument");
+    *count = 0;
+    if (!s->rec3) return FVB_OK;  // aux holds other families' own quantities
+    unsigned long long v = 0;
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(&v, &s->ctrl->aux, sizeof v, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "limiter count");
+    *count = (int64_t)v;
+    return FVB_OK;
+}
+
 fvb_status fvb_set_d2av(fvb_solver *s, double c2, double cg, double sc)
 {
     if (!s) return fail(FVB_ERR_INVALID, "null argument");

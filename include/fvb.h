@@ -199,6 +199,12 @@ FVB_API fvb_status fvb_advance(fvb_solver *s, double t_stop, int64_t max_steps, 
 /* Wait for the stream and read the step control (t, dt, lam_max, status). */
 FVB_API fvb_status fvb_sync(fvb_solver *s, fvb_stats *st);
 
+/* The rec3 family's count of 2x2 blocks whose mean itself needed the floor
+ * fix (the "brutal mean-fix activations" fv_rec3_2d.cu:250, :594 reports),
+ * since the state was last set; 0 for the other flux families.  Waits for
+ * the solver's stream. */
+FVB_API fvb_status fvb_limiter_fixes(fvb_solver *s, int64_t *count);
+
 /* Coefficients of the FVB_FLUX_UP_HLLC_D2AV viscosity: C2 (Ducros-gated),
  * Cg (global, weight 1 - S_D) and the sensor's sound-speed scale sc; the
  * .bak's command-line arguments 2-4, defaults 0.5, 0, 0.05

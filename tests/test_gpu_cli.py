@@ -193,3 +193,35 @@ def test_device_frame_fields_match_host_restatement(case, bc, prec):
     scale = max(float(np.abs(ref["vorticity"]).max()), 1e-6)
     assert np.abs(fr["vorticity"] - ref["vorticity"]).max() <= 1e-5 * scale
     assert s.sync().steps == 27
+
+
+def test_fvb_rec3_matches_the_oracle(tmp_path):
+    """fvb_rec3 (fv_rec3's command line): step count, the limiter's mean-fix
+    count and the L2 errors / minimum density it prints, against the oracle
+    run to the same time"""
+    import re
+    import oracle as O
+    for case, args, t_end in (("pv", ["32", "pv"], 0.3), ("sod", ["32"], 0.05)):
+        r = subprocess.run([str(BIN / "fvb_rec3"), *args, "--t-end", str(t_end)], cwd=tmp_path,
+                           capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        out = r.stdout
+        steps = int(re.search(r"Done: (\d+) steps", out).group(1))
+        fixes = int(re.search(r"brutal mean-fix activations: (\d+)", out).group(1))
+        assert "conservation drift: mass" in out
+        L = 10.0 if case == "pv" else 1.0
+        n, h = 32, L / 32
+        U = O.rec3_ic(n, h, case)
+        brutal0 = O.rec3_limit(U, n)
+        O.bc(U, n, 2, 1)
+        st, t, k, lmax, dt, brutal = O.rec3_run(U, n, h, 0.4, 10 ** 6, t_stop=t_end)
+        assert st == 0 and k == steps and fixes == brutal0 + brutal
+        if case == "pv":
+            e_rho, e_vel = O.rec3_err(U, n, h, "pv")
+            got_rho = float(re.search(r"L2\(rho\) = (\S+)", out).group(1))
+            got_vel = float(re.search(r"L2\(vel\) = (\S+)", out).group(1))
+            assert got_rho == pytest.approx(e_rho, rel=1e-5) and got_vel == pytest.approx(e_vel, rel=1e-5)
+        else:
+            rmin = float(U[0, 2:-2, 2:-2].min())
+            got = float(re.search(r"final min rho = (\S+)", out).group(1))
+            assert got == pytest.approx(rmin, rel=1e-3)
