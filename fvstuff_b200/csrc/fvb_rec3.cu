@@ -10,10 +10,12 @@
 // non-overlapping 2x2 blocks of the new state (block corners by bilinear
 // extrapolation, one common theta per block, block total conserved).
 //
-// One launch per stage does all of it for a tile of 32 x 16 cells: tiles
-// start on even cells, so every 2x2 block lies in one tile and the limiter
-// runs in shared memory before the stores (interior + periodic ghost
-// images), and stage 3 max-reduces the wave speed of the limited state.
+// One launch per stage does all of it for a tile of 32 x 32 cells: tiles
+// start on even cells, so every 2x2 block lies in one tile, and after the
+// face fluxes one thread takes one block -- the residuals and RK values of
+// its four cells, the limiter, the stores (interior + periodic ghost
+// images) -- with no barrier between; stage 3 max-reduces the wave speed of
+// the limited state.
 //
 // The reference scatters each face flux into its two cells with atomicAdd;
 // here every cell gathers its four face terms in the order a serial run of
@@ -29,7 +31,7 @@ namespace fvb {
 namespace {
 
 constexpr double R3_GAM = 1.4, R3_PFLOOR = 1e-9, R3_RHOFLOOR = 1e-12;
-constexpr int RTX = 32, RTY = 16, RNT = 256, RG = 2;
+constexpr int RTX = 32, RTY = 32, RNT = 256, RG = 2;
 constexpr int RSW = RTX + 2 * RG, RSH = RTY + 2 * RG, RPL = RSW * RSH;
 constexpr int RNC = RTX * RTY;
 
@@ -183,7 +185,6 @@ __global__ void __launch_bounds__(RNT, 2) rec3_stage_kernel(const GridDev gd, in
     double *Q = reinterpret_cast<double *>(smem_raw);  // [4][RSH][RSW] stage input
     double *FX = Q + 4 * RPL;                          // [4][RTY][RTX+1]
     double *FY = FX + 4 * RTY * (RTX + 1);             // [4][RTY+1][RTX]
-    double *NW = FY + 4 * (RTY + 1) * RTX;             // [4][RTY][RTX] new state
     __shared__ TileCtl s_ctl;
     __shared__ double s_red[RNT / 32];
     const int tid = threadIdx.x, n = gd.n, np = n + 2 * RG;
@@ -241,55 +242,41 @@ __global__ void __launch_bounds__(RNT, 2) rec3_stage_kernel(const GridDev gd, in
             o[0] = Fn[0]; o[QN * os] = Fn[1]; o[QT * os] = Fn[2]; o[3 * os] = Fn[3];
         }
         __syncthreads();
-        // ---- residual in the serial scatter's order, RK combination -------
-        for (int k = tid; k < RNC; k += RNT) {
-            const int r = k / RTX, c = k - r * RTX, i = tx0 + c, j = ty0 + r;
-            if (i >= n || j >= n) continue;
-            const long long e = r3_at(gd, j, i);
-            for (int q = 0; q < 4; ++q) {
-                const double *fx = FX + q * RTY * (RTX + 1) + r * (RTX + 1) + c;
-                const double *fy = FY + q * (RTY + 1) * RTX + r * RTX + c;
-                const double tl = fx[0] * inv_h, tr = -fx[1] * inv_h;      // left face in, right face out
-                const double tb = fy[0] * inv_h, tt = -fy[RTX] * inv_h;    // bottom in, top out
-                double L;
-                if (i > 0 && j > 0) L = ((tb + tl) + tr) + tt;
-                else if (i == 0 && j > 0) L = ((tb + tr) + tt) + tl;
-                else if (i > 0) L = ((tl + tr) + tt) + tb;
-                else L = ((tr + tt) + tl) + tb;
-                const double qa = u0[e + q * gd.plane];
-                const double qb = Q[q * RPL + (r + RG) * RSW + (c + RG)];
-                NW[q * RNC + k] = ca * qa + cb * (qb + ctl.dt * L);
-            }
-        }
-        __syncthreads();
-        // ---- 2x2-block positivity limiter on the new state ----------------
+        // ---- per 2x2 block, one thread: residual of its four cells in the
+        //      serial scatter's order, RK combination, the block limiter,
+        //      stores with the periodic ghost images, stage-3 wave speed -----
         for (int kb = tid; kb < RNC / 4; kb += RNT) {
             const int jb = kb / (RTX / 2), ib = kb - jb * (RTX / 2);
             const int c0 = 2 * ib, r0 = 2 * jb;
             if (tx0 + c0 >= n || ty0 + r0 >= n) continue;  // n even: the block is whole
             double U[4][4];
             for (int cc = 0; cc < 4; cc++) {
-                const int kk = (r0 + (cc >> 1)) * RTX + c0 + (cc & 1);
-                for (int q = 0; q < 4; q++) U[cc][q] = NW[q * RNC + kk];
-            }
-            if (r3_limit_block(U, &brutal))
-                for (int cc = 0; cc < 4; cc++) {
-                    const int kk = (r0 + (cc >> 1)) * RTX + c0 + (cc & 1);
-                    for (int q = 0; q < 4; q++) NW[q * RNC + kk] = U[cc][q];
+                const int r = r0 + (cc >> 1), c = c0 + (cc & 1), i = tx0 + c, j = ty0 + r;
+                const long long e = r3_at(gd, j, i);
+                for (int q = 0; q < 4; ++q) {
+                    const double *fx = FX + q * RTY * (RTX + 1) + r * (RTX + 1) + c;
+                    const double *fy = FY + q * (RTY + 1) * RTX + r * RTX + c;
+                    const double tl = fx[0] * inv_h, tr = -fx[1] * inv_h;      // left face in, right face out
+                    const double tb = fy[0] * inv_h, tt = -fy[RTX] * inv_h;    // bottom in, top out
+                    double L;
+                    if (i > 0 && j > 0) L = ((tb + tl) + tr) + tt;
+                    else if (i == 0 && j > 0) L = ((tb + tr) + tt) + tl;
+                    else if (i > 0) L = ((tl + tr) + tt) + tb;
+                    else L = ((tr + tt) + tl) + tb;
+                    const double qa = u0[e + q * gd.plane];
+                    const double qb = Q[q * RPL + (r + RG) * RSW + (c + RG)];
+                    U[cc][q] = ca * qa + cb * (qb + ctl.dt * L);
                 }
-        }
-        __syncthreads();
-        // ---- stores with the periodic ghost images; stage-3 wave speed ----
-        for (int k = tid; k < RNC; k += RNT) {
-            const int r = k / RTX, c = k - r * RTX, i = tx0 + c, j = ty0 + r;
-            if (i >= n || j >= n) continue;
-            double v[4];
-            for (int q = 0; q < 4; ++q) v[q] = NW[q * RNC + k];
-            put_cell<double>(gd, out, j, i, v);
-            if (stage == 3) {
-                double W[4];
-                r3_w(v, W);
-                lacc = fmax(lacc, fabs(W[1]) + fabs(W[2]) + r3_snd(W[0], W[3]));
+            }
+            r3_limit_block(U, &brutal);
+            for (int cc = 0; cc < 4; cc++) {
+                const int i = tx0 + c0 + (cc & 1), j = ty0 + r0 + (cc >> 1);
+                put_cell<double>(gd, out, j, i, U[cc]);
+                if (stage == 3) {
+                    double W[4];
+                    r3_w(U[cc], W);
+                    lacc = fmax(lacc, fabs(W[1]) + fabs(W[2]) + r3_snd(W[0], W[3]));
+                }
             }
         }
         if (stage == 3 && tid == 0 && t == 0) leader_finish<P64>(gd.ctrl);
@@ -416,7 +403,7 @@ __global__ void rec3_ic_kernel(const GridDev gd, double *buf, int icase, double 
 
 size_t rec3_smem()
 {
-    return sizeof(double) * (4 * RPL + 4 * RTY * (RTX + 1) + 4 * (RTY + 1) * RTX + 4 * RNC);
+    return sizeof(double) * (4 * RPL + 4 * RTY * (RTX + 1) + 4 * (RTY + 1) * RTX);
 }
 
 int sm_count()
