@@ -191,6 +191,33 @@ def test_vortex_256_matches_reference_cuda_kernels():
 
 
 @pytest.mark.skipif(not O.have_ref_gpu(), reason="reference GPU build absent")
+def test_vortex_256_full_period_against_reference_and_exact():
+    """The whole configuration-1 run: one period (t = 10, about 2200 steps)
+    on the plain FP64 path and on the reference's own FP64 kernels, both
+    landing on t = 10; prints their difference (which grows from the
+    last-bit level of the first steps) and both errors against the exact
+    solution (the initial vortex)."""
+    n = 256
+    w0 = vortex(n)
+    U = _padded(w0, 1)
+    ref = U.copy()
+    status, t, k, lmax, dt, ms = O.refg_up_run(ref, n, 10.0 / n, 0.5, 1, 10 ** 6, t_stop=10.0)
+    assert status == 0 and abs(t - 10.0) < 1e-12
+    s = F.Solver(n, bc="periodic", x0=-5, y0=-5, length=10.0, cfl=0.5)
+    s.set_state(U)
+    st = s.advance(10.0)
+    assert st.status == 0 and st.steps == k and abs(st.t - 10.0) < 1e-12
+    got = s.get_state()
+    err = rel_linf(_cons(got), _cons(ref))
+    got, want = got[:, 4:-4, 4:-4], ref[:, 4:-4, 4:-4]
+    l2 = lambda w: float(np.sqrt(np.mean((w[0] - w0[0]) ** 2)))
+    print("vortex 256^2, one period (%d steps): rel L-inf vs reference kernels %.3e; L2(rho) vs exact "
+          "%.4e (fvb) / %.4e (reference)" % (k, err, l2(got), l2(want)))
+    assert err <= TOL64
+    assert abs(l2(got) - l2(want)) <= 1e-6 * l2(want)
+
+
+@pytest.mark.skipif(not O.have_ref_gpu(), reason="reference GPU build absent")
 def test_f32_mode_matches_shipped_fp32_kernels():
     """FVB_PREC_F32 reproduces the solver as shipped (float state, double
     reconstruction arithmetic) against its own FP32 kernels."""
