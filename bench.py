@@ -598,7 +598,7 @@ def run_families(args):
 
 
 def _density_errors(a, b):
-    """relative L1 and L-inf of density a against b (interior arrays)"""
+    """relative L1 and L-inf of a field a against b (interior arrays)"""
     d = np.abs(a - b)
     return float(d.sum() / np.abs(b).sum()), float(d.max() / np.abs(b).max())
 
@@ -626,10 +626,16 @@ def run_precision(args):
     for k in range(1, 11):
         t = t_end * k / 10
         sa, sb, sc = a.advance(t), b.advance(t), c.advance(t)
-        ra = a.get_state(interior=True)[0]
-        l1, linf = _density_errors(b.get_state(interior=True)[0], ra)
+        ca = a.get_state(layout="cons", interior=True)
+        cb = b.get_state(layout="cons", interior=True)
+        ra = ca[0]
+        l1, linf = _density_errors(cb[0], ra)
         p1, pinf = _density_errors(c.get_state(interior=True)[0], ra)
+        # every conserved variable (rho, rho u, rho v, E): L1 and L-inf relative
+        per_var = {name: dict(zip(("l1_rel", "linf_rel"), _density_errors(cb[q], ca[q])))
+                   for q, name in enumerate(("rho", "rho_u", "rho_v", "E"))}
         curve.append({"t": t, "l1_rel": l1, "linf_rel": linf, "f64_1ulp_l1_rel": p1, "f64_1ulp_linf_rel": pinf,
+                      "conserved": per_var,
                       "steps_f64": sa.steps, "steps_f32c": sb.steps, "status": [sa.status, sb.status, sc.status]})
         print("KH %d^2 t=%.2f: FP32c L1 %.3e Linf %.3e | FP64 1-ulp start L1 %.3e Linf %.3e (steps %d / %d)"
               % (n, t, l1, linf, p1, pinf, sa.steps, sb.steps), file=sys.stderr, flush=True)
