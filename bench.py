@@ -160,11 +160,11 @@ def traffic_from_profiles(precision: str, n: int):
 # ---------------------------------------------------------------------------
 # CPU: the reference's own kernels compiled for the host (oracle/_ref)
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(sample_n: int, steps: int, warmup: int):
+def cpu_reference_rate(sample_n: int, steps: int, warmup: int, threads: int | None = None):
     import oracle as O
     sys.path.insert(0, str(ROOT / "tests"))
     from cases import kh, pad
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     O.ref_set_threads(threads)
     kind = "reference" if O.have_ref_host() else "port"
     U = pad(kh(sample_n), 4)
@@ -190,6 +190,8 @@ def run_reference(args):
     sample = min(args.n, 512)
     steps = max(1, min(args.steps, 20))
     rate, kind, threads, sec = cpu_reference_rate(sample, steps, min(args.warmup, 2))
+    # the same kernels on one host thread, a smaller sample
+    rate1, _, _, sec1 = cpu_reference_rate(256, 4, 1, threads=1)
     line = {"metric": METRIC, "value": rate, "unit": "cell-stage updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -197,7 +199,9 @@ def run_reference(args):
             "cpu_baseline": {"value": rate, "unit": "cell-stage updates/s", "cores": threads, "kind": kind,
                              "sample": "%d steps of the same KH case on a %dx%d grid (FP64 retype of "
                                        "fv_up7_ducros_2d.cu kernels, OpenMP over all host threads)"
-                                       % (steps, sample, sample)},
+                                       % (steps, sample, sample),
+                             "single_thread": {"value": rate1, "cores": 1,
+                                               "sample": "4 steps on a 256x256 grid"}},
             "e2e": {"value": rate, "unit": "cell-stage updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
