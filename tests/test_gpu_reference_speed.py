@@ -95,3 +95,77 @@ def test_keep_faster_than_reference_kernels():
                                                             ms, 3.0 * n * n * steps / ms / 1e6, ms_ref / ms, err))
     assert st.status == 0 and st.steps == steps
     assert ms < ms_ref
+
+
+def _ours_rate(n, precision, w, steps=None, t_stop=None, **kw):
+    """cell-stage updates/s of this library on a prepared primitive state"""
+    import torch
+    stream = torch.cuda.Stream()
+    s = F.Solver(n, bc="periodic", cfl=0.5, precision=precision, stream=stream.cuda_stream, **kw)
+    s.set_state(w, interior=True)
+    s.step(2)
+    s.sync()
+    s.set_state(w, interior=True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    if t_stop is not None:
+        s.advance(t_stop)   # (fvb_step would enqueue every one of its steps)
+    else:
+        s.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    st = s.sync()
+    s.close()
+    return 3.0 * n * n * st.steps / (e0.elapsed_time(e1) / 1e3), st.steps
+
+
+def test_baseline_table_configs_1_and_5():
+    """The rates of the baseline table: configuration 1 (vortex 256^2, one
+    period) and 5 (KH 8192^2, 20 steps) on the reference's GPU kernels (FP32
+    as shipped, FP64 retype), on its kernels built for the host (all threads
+    and one), and on this library; prints the table."""
+    from cases import vortex
+    rows = []
+    # configuration 1
+    n = 256
+    w = vortex(n)
+    U = pad(w, 4)
+    O.bc(U, n, 4, 1)
+    for dtype, tag in ((np.float32, "B1 reference GPU, FP32"), (np.float64, "B2 reference GPU, FP64")):
+        st, t, k, lmax, dt, ms = O.refg_up_run(U.astype(dtype), n, 10.0 / n, 0.5, 1, 10 ** 6, t_stop=10.0)
+        assert st == 0
+        rows.append(("1", tag, 3.0 * n * n * k / (ms / 1e3)))
+    for threads, tag in ((0, "B3 reference host, all threads"), (1, "B3 reference host, 1 thread")):
+        O.ref_set_threads(threads)
+        V = U.copy()
+        import time
+        t0 = time.perf_counter()
+        O.ref_up_run(V, n, 10.0 / n, 0.5, 1, 1)
+        t1 = time.perf_counter()
+        O.ref_up_run(V, n, 10.0 / n, 0.5, 1, 4)
+        t2 = time.perf_counter()
+        rows.append(("1", tag, 3.0 * n * n * 3 / ((t2 - t1) - (t1 - t0))))
+    O.ref_set_threads(0)
+    ours, k = _ours_rate(n, "f64", w, t_stop=10.0, x0=-5.0, y0=-5.0, length=10.0)
+    rows.append(("1", "fvb plain FP64", ours))
+    # configuration 5
+    n, steps = 8192, 20
+    w = kh(n)
+    U = pad(w, 4)
+    O.bc(U, n, 4, 1)
+    ref = {}
+    for dtype, tag in ((np.float32, "B1 reference GPU, FP32"), (np.float64, "B2 reference GPU, FP64")):
+        st, t, k, lmax, dt, ms = O.refg_up_run(U.astype(dtype), n, 1.0 / n, 0.5, 1, steps)
+        assert st == 0 and k == steps
+        ref[dtype] = 3.0 * n * n * steps / (ms / 1e3)
+        rows.append(("5", tag, ref[dtype]))
+    del U
+    for prec in ("f64", "f32c"):
+        r, _ = _ours_rate(n, prec, w, steps=steps)
+        rows.append(("5", "fvb " + prec, r))
+    print("\nconfig  arm                              G cell-stages/s")
+    for c, tag, r in rows:
+        print("  %s     %-32s %9.4f" % (c, tag, r / 1e9))
+    assert rows[-2][2] > ref[np.float64] and rows[-1][2] > ref[np.float32]
