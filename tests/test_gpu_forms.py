@@ -164,6 +164,41 @@ def test_batch_join_midway_and_budget():
     assert i3 >= 0
 
 
+@pytest.mark.parametrize("prec", ["f32c", "f64"])
+def test_batch_bad_instances_stay_isolated(prec):
+    """instances whose initial state is not a state -- NaN density,
+    negative density and pressure -- run as the reference's scheme runs them
+    (its floors turn NaN and negative rho, p into 1e-14, its sound-speed
+    clamp a NaN c^2 into 1e-14; a non-positive wave speed stops the
+    instance); whatever they do, the good instances of the same batch finish
+    exactly as they do alone"""
+    b = F.Batch(precision=prec)
+    good = []
+    for k, n in enumerate((48, 64, 40)):
+        d, c = _desc(n, 300 + k, 0.03)
+        good.append((b.add(d), n, c))
+    bad = []
+    for n, params in ((56, dict(rho=float("nan"))), (32, dict(rho=-1.0, p=-1.0))):
+        c = F.case_params("uniform", 0.0, 0.0, 1.0, **params)
+        bad.append(b.add(F.Batch.desc(n, c, 0.03, bc="transmissive", cfl=0.5)))
+    done = set()
+    for _ in range(400):
+        b.run(8)
+        done.update(b.poll())
+        if len(done) == 5:
+            break
+    assert len(done) == 5
+    for iid in bad:
+        assert b.stats(iid).status in (0, F._lib.ERR_BLOWUP, F._lib.ERR_DT_UNDERFLOW)
+    for iid, n, c in good:
+        st = b.stats(iid)
+        assert st.status == 0 and st.t == pytest.approx(0.03, rel=0, abs=1e-12)
+        s = F.Solver(n, precision=prec, bc="transmissive", cfl=0.5)
+        s.init_case(c)
+        s.advance(0.03)
+        assert np.array_equal(b.get_state(iid, n), s.get_state(interior=True))
+
+
 # --- serving loop ---------------------------------------------------------------
 
 def test_serve_stream_matches_alone():

@@ -363,3 +363,56 @@ def test_riemann_variants_match_oracle(riemann, bc, n, case):
 def test_riemann_variant_rejects_other_forms():
     with pytest.raises(F.FvbError):
         F.Solver(64, flux="up_ducros_roe", precision="f32c")
+
+
+# --- guard bands: nothing is written outside the caller's arrays ----------------
+
+SENTINEL = 12345.678
+
+
+def _guarded(count, dtype, guard=4096):
+    """a device array of `count` elements between two sentinel-filled guards"""
+    big = torch.full((guard + count + guard,), SENTINEL, dtype=dtype, device="cuda")
+    return big, big[guard:guard + count]
+
+
+def _guards_intact(big, count, guard=4096):
+    torch.cuda.synchronize()
+    g = torch.cat([big[:guard], big[guard + count:]])
+    return bool(torch.all(g == SENTINEL).item())
+
+
+@pytest.mark.parametrize("n", [8, 13, 37])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_kernel_contract_writes_stay_in_bounds(n, dtype):
+    """the kernel-level entry points on ragged sizes write only inside their
+    output arrays (guard bands of a sentinel value on both sides), and
+    apply_bc / rk3_stage leave the parts they do not own untouched"""
+    npd = n + 8
+    U = torch.from_numpy(_padded(smooth(n, seed=n), 1)).to(dtype).cuda().contiguous()
+    big_r, rhs = _guarded(4 * n * n, dtype)
+    big_l, lam = _guarded(n * n, dtype)
+    F.up_rhs(U, rhs.view(4, n, n), lam.view(n, n), n, npd, 1.0 / n)
+    assert _guards_intact(big_r, 4 * n * n) and _guards_intact(big_l, n * n)
+    # apply_bc on a guarded copy: the interior is not touched
+    big_q, Q = _guarded(4 * npd * npd, dtype)
+    Q.copy_(U.reshape(-1))
+    F.apply_bc(Q.view(4, npd, npd), n, npd, "periodic")
+    assert _guards_intact(big_q, 4 * npd * npd)
+    assert torch.equal(Q.view(4, npd, npd)[:, 4:-4, 4:-4], U[:, 4:-4, 4:-4])
+    # rk3_stage writes the interior of Uo only
+    big_o, Uo = _guarded(4 * npd * npd, dtype)
+    Uo.fill_(-7.0)
+    F.rk3_stage(2, Uo.view(4, npd, npd), U, U, rhs.view(4, n, n), 1e-3, n, npd)
+    assert _guards_intact(big_o, 4 * npd * npd)
+    V = Uo.view(4, npd, npd)
+    ring = torch.ones((npd, npd), dtype=torch.bool, device="cuda")
+    ring[4:-4, 4:-4] = False
+    assert bool(torch.all(V[:, ring] == -7.0).item())
+    # the solver's state export to a device array
+    s = F.Solver(n, bc="periodic")
+    s.set_state(U.cpu().numpy())
+    s.step(3)
+    big_s, out = _guarded(4 * n * n, torch.float64)
+    s.get_state(interior=True, out=out.view(4, n, n))
+    assert _guards_intact(big_s, 4 * n * n)
