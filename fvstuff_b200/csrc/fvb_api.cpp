@@ -448,6 +448,7 @@ int fvb_ghost_width(const fvb_solver *s) { return s ? s->g : 0; }
 
 fvb_status fvb_init_case(fvb_solver *s, const fvb_case *c)
 {
+    NvtxRange nvtx_range("fvb_init_case");
     if (!s || !c) return fail(FVB_ERR_INVALID, "null argument");
     if (c->kind >= FVB_CASE_REC3_SOD && c->kind <= FVB_CASE_GRESHO) {
         if (!s->rec3) return fail(FVB_ERR_INVALID, "case %d is a rec3 case (FVB_FLUX_REC3)", c->kind);
@@ -472,6 +473,7 @@ fvb_status fvb_init_case(fvb_solver *s, const fvb_case *c)
 
 fvb_status fvb_set_state(fvb_solver *s, const void *src, int layout, int dtype, int where, int interior_only)
 {
+    NvtxRange nvtx_range("fvb_set_state");
     if (!s || !src) return fail(FVB_ERR_INVALID, "null argument");
     if ((layout != 0 && layout != 1) || (dtype != 0 && dtype != 1) || (where != 0 && where != 1))
         return fail(FVB_ERR_INVALID, "bad layout/dtype/where");
@@ -501,6 +503,7 @@ fvb_status fvb_set_state(fvb_solver *s, const void *src, int layout, int dtype, 
 
 fvb_status fvb_get_state(fvb_solver *s, void *dst, int layout, int dtype, int where, int interior_only)
 {
+    NvtxRange nvtx_range("fvb_get_state");
     if (!s || !dst) return fail(FVB_ERR_INVALID, "null argument");
     if ((layout != 0 && layout != 1) || (dtype != 0 && dtype != 1) || (where != 0 && where != 1))
         return fail(FVB_ERR_INVALID, "bad layout/dtype/where");
@@ -564,6 +567,7 @@ fvb_status fvb_debug_drop_load(fvb_solver *s)
 
 fvb_status fvb_frame_begin(fvb_solver *s)
 {
+    NvtxRange nvtx_range("fvb_frame_begin");
     if (!s) return fail(FVB_ERR_INVALID, "null argument");
     const size_t n2 = (size_t)s->n * s->n, np2 = (size_t)s->G.np * s->G.np;
     cudaError_t e = cudaSuccess;
@@ -708,6 +712,7 @@ fvb_status fvb_get_state_hilo(fvb_solver *s, float *hi, float *lo)
 
 fvb_status fvb_step(fvb_solver *s, int nsteps, double t_stop)
 {
+    NvtxRange nvtx_range("fvb_step");
     if (!s || nsteps < 0) return fail(FVB_ERR_INVALID, "bad argument");
     cudaError_t e = ctrl_set(s->ctrl, t_stop, 0, 0, 0, 0, s->stream);
     if (e == cudaSuccess) e = enqueue_steps(s, nsteps);
@@ -737,6 +742,7 @@ fvb_status fvb_sync(fvb_solver *s, fvb_stats *st)
 
 fvb_status fvb_advance(fvb_solver *s, double t_stop, int64_t max_steps, int chunk)
 {
+    NvtxRange nvtx_range("fvb_advance");
     if (!s) return fail(FVB_ERR_INVALID, "null solver");
     int64_t done = 0;
     for (;;) {

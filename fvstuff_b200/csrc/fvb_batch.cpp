@@ -353,6 +353,7 @@ fvb_status fvb_batch_add(fvb_batch *b, const fvb_instance_desc *d, int *id)
 
 fvb_status fvb_batch_run(fvb_batch *b, int nsteps)
 {
+    NvtxRange nvtx_range("fvb_batch_run");
     if (!b || nsteps < 0) return fail(FVB_ERR_INVALID, "bad argument");
     if (b->dirty) {
         fvb_status st = upload_table(b);
@@ -374,6 +375,7 @@ fvb_status fvb_batch_run(fvb_batch *b, int nsteps)
 
 fvb_status fvb_batch_poll(fvb_batch *b, int *ids, int cap, int *n_done)
 {
+    NvtxRange nvtx_range("fvb_batch_poll");
     if (!b || !n_done) return fail(FVB_ERR_INVALID, "null argument");
     *n_done = 0;
     cudaError_t e = cudaMemcpyAsync(b->ctrl_host, b->ctrl_dev, sizeof(Ctrl) * b->max_inst, cudaMemcpyDeviceToHost,

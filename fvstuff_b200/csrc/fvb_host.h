@@ -2,6 +2,8 @@
 #pragma once
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "fvb_aux.h"
 
 namespace fvb {
@@ -14,6 +16,15 @@ struct Geometry {
     size_t elem;   // bytes per state word
     int nbuf;      // padded 4-variable buffers (3: state + 2 stage outputs; 6 for F32C)
     size_t bytes;  // all buffers
+};
+
+// A named range on a profiler's timeline (Nsight Systems / Compute) around a
+// host entry point; without a profiler attached it costs next to nothing.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
 };
 
 fvb_status fail(fvb_status st, const char *fmt, ...);

@@ -22,6 +22,7 @@ using clk = std::chrono::steady_clock;
 extern "C" fvb_status fvb_serve_run(const fvb_serve_config *cfg, const fvb_request *reqs, int nreq,
                                     fvb_request_result *res, double *wall_seconds)
 {
+    NvtxRange nvtx_range("fvb_serve_run");
     if (!cfg || (!reqs && nreq) || (!res && nreq) || nreq < 0) return fail(FVB_ERR_INVALID, "bad argument");
     fvb_batch *b = nullptr;
     fvb_status st = fvb_batch_create(&cfg->batch, &b);
