@@ -95,7 +95,7 @@ class Solver:
     """One N x N grid advanced by the fused SSP-RK3 stage kernels.
 
     Parameters mirror fvb_config: ``n`` cells per side on
-    ``[x0, x0+length] x [y0, y0+length]``, ``order`` (3/5/7), ``flux``
+    ``[x0, x0+length] x [y0, y0+length]``, ``order`` (3/5/7/9), ``flux``
     ('up_ducros' | 'up_ducros_hll' | 'up_ducros_roe' | 'keep' | 'rec3' |
     'up_hllc_d2av'), ``precision`` ('f64' | 'f32' | 'f32c'),
     ``bc`` / ``bc_y`` ('reflect' | 'periodic' | 'transmissive'), ``gamma``,

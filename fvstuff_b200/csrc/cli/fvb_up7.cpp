@@ -2,7 +2,7 @@
 // main, :886-1067) on libfvb.
 //
 //   fvb_up7 [N] [--cfl C] [--t-end T] [--case sod|vortex|kh|riemann4]
-//           [--gamma G] [--bc reflect|periodic|transmissive] [--order 3|5|7]
+//           [--gamma G] [--bc reflect|periodic|transmissive] [--order 3|5|7|9]
 //           [--precision f64|f32|f32c] [--frames F] [--prefix P] [--seed S]
 //           [--bin] [--no-ppm] [--save FILE] [--resume FILE]
 //   fvb_up7 --d2av [N [C2 [Cg [sc [order]]]]] [options above]

@@ -326,10 +326,10 @@ fvb_status fvb_create(const fvb_config *cfg, fvb_solver **out)
     if (cfg->precision < 0 || cfg->precision > 2) return fail(FVB_ERR_INVALID, "unknown precision %d", cfg->precision);
     if (keep && cfg->precision != FVB_PREC_F64)
         return fail(FVB_ERR_INVALID, "the KEEP flux family runs in FP64 (as keep_fv_euler_2d.cu)");
-    if (!keep && !rec3 && !(cfg->order == 3 || cfg->order == 5 || cfg->order == 7))
-        return fail(FVB_ERR_INVALID, "order must be 3, 5 or 7 (got %d)", cfg->order);
+    if (!keep && !rec3 && !(cfg->order == 3 || cfg->order == 5 || cfg->order == 7 || cfg->order == 9))
+        return fail(FVB_ERR_INVALID, "order must be 3, 5, 7 or 9 (got %d)", cfg->order);
     if (!keep && !rec3 && cfg->precision != FVB_PREC_F64 && cfg->order != 7)
-        return fail(FVB_ERR_INVALID, "orders 3 and 5 are built for FP64 only");
+        return fail(FVB_ERR_INVALID, "orders 3, 5 and 9 are built for FP64 only");
     const int g = (keep || rec3) ? 2 : d2av ? d2av_ghost(cfg->order) : (cfg->order + 1) / 2;
     if (cfg->n < g || cfg->n > 65536) return fail(FVB_ERR_INVALID, "n = %d out of range [%d, 65536]", cfg->n, g);
     for (int b : {cfg->bc_x, cfg->bc_y})
@@ -809,7 +809,7 @@ fvb_status fvb_up_rhs(const void *Qp, void *rhs, void *lam, int n, int np, int o
                       int dtype, void *stream)
 {
     if (!Qp || !rhs || !lam) return fail(FVB_ERR_INVALID, "null argument");
-    if (order != 7 && !(dtype == FVB_F64 && (order == 3 || order == 5)))
+    if (order != 7 && !(dtype == FVB_F64 && (order == 3 || order == 5 || order == 9)))
         return fail(FVB_ERR_INVALID, "order %d not built for this dtype", order);
     const int g = (order + 1) / 2;
     if (n < 1 || np < n + 2 * g) return fail(FVB_ERR_INVALID, "np must be >= n + 2g");

@@ -1,5 +1,5 @@
 // fvb_d2av.cu -- the scheme kept in fv_up7_ducros_2d.cu.bak (the earlier
-// form of fv_up7) on the device: UP-order (3, 5, 7) reconstruction of the
+// form of fv_up7) on the device: UP-order (3, 5, 7, 9) reconstruction of the
 // conserved variables, HLLC on the reconstructed states, and a D2
 // artificial viscosity
 //   D2 = (C2/h) S_D (sum of lam_face dU) + (Cg/h) (1 - S_D) (the same sum)
@@ -85,6 +85,15 @@ __device__ __forceinline__ void d2_recon(const double *s, double &vL, double &vR
     } else if constexpr (ORDER == 5) {
         vL = (2.0 * s[0] - 13.0 * s[1] + 47.0 * s[2] + 27.0 * s[3] - 3.0 * s[4]) / 60.0;
         vR = (-3.0 * s[1] + 27.0 * s[2] + 47.0 * s[3] - 13.0 * s[4] + 2.0 * s[5]) / 60.0;
+    } else if constexpr (ORDER == 9) {
+        // the published weights as they stand (the left-biased set sums to
+        // 4217/2520)                            fv_up7_ducros_2d.cu.bak:132-142
+        vL = (3.0 * s[0] - 25.0 * s[1] + 101.0 * s[2] - 319.0 * s[3] + 2765.0 * s[4] + 2139.0 * s[5] -
+              533.0 * s[6] + 97.0 * s[7] - 11.0 * s[8]) /
+             2520.0;
+        vR = (-11.0 * s[1] + 97.0 * s[2] - 533.0 * s[3] + 2139.0 * s[4] + 2765.0 * s[5] - 319.0 * s[6] +
+              101.0 * s[7] - 25.0 * s[8] + 3.0 * s[9]) /
+             2520.0;
     } else {
         vL = (-3.0 * s[0] + 25.0 * s[1] - 101.0 * s[2] + 319.0 * s[3] + 214.0 * s[4] - 38.0 * s[5] + 4.0 * s[6]) /
              420.0;
@@ -102,7 +111,8 @@ struct D2Shape {
     // Q[4][PL] | SU, SV, LX, LY, CS [PL each] | FX[4][NFX] | FY[4][NFY]
     static constexpr size_t SMEM = sizeof(double) * (9 * PL + 4 * NFX + 4 * NFY);
     // resident CTAs an SM is compiled for: four (56 KB each, <= 64
-    // registers) with the 3-cell halo, three (64 KB) with UP7's 4
+    // registers) with the 3-cell halo, three (64 KB, 72 KB) with UP7's 4
+    // and UP9's 5
     static constexpr int MINB = HB == 3 ? 4 : 3;
 };
 
@@ -364,6 +374,7 @@ cudaError_t d2av_launch_stage(const GridDev &gd, int order, int stage, int tiles
     if (order == 3) return launch_order<3>(gd, stage, tiles, av, s);
     if (order == 5) return launch_order<5>(gd, stage, tiles, av, s);
     if (order == 7) return launch_order<7>(gd, stage, tiles, av, s);
+    if (order == 9) return launch_order<9>(gd, stage, tiles, av, s);
     return cudaErrorInvalidValue;
 }
 

@@ -95,8 +95,15 @@ __device__ __forceinline__ void upface(const R *s, R &vL, R &vR)
     } else if constexpr (ORDER == 5) {
         vL = R((RR(2.0) * s[0] - RR(13.0) * s[1] + RR(47.0) * s[2] + RR(27.0) * s[3] - RR(3.0) * s[4]) / RR(60.0));
         vR = R((-RR(3.0) * s[1] + RR(27.0) * s[2] + RR(47.0) * s[3] - RR(13.0) * s[4] + RR(2.0) * s[5]) / RR(60.0));
+    } else if constexpr (ORDER == 9) {
+        // the published UP9 weights, as they stand (the left-biased set sums
+        // to 4217/2520, not one)                 fv_up7_ducros_2d.cu:176-186
+        vL = R((RR(3.0) * s[0] - RR(25.0) * s[1] + RR(101.0) * s[2] - RR(319.0) * s[3] + RR(2765.0) * s[4]
+                + RR(2139.0) * s[5] - RR(533.0) * s[6] + RR(97.0) * s[7] - RR(11.0) * s[8]) / RR(2520.0));
+        vR = R((-RR(11.0) * s[1] + RR(97.0) * s[2] - RR(533.0) * s[3] + RR(2139.0) * s[4] + RR(2765.0) * s[5]
+                - RR(319.0) * s[6] + RR(101.0) * s[7] - RR(25.0) * s[8] + RR(3.0) * s[9]) / RR(2520.0));
     } else {
-        static_assert(ORDER == 7, "ORDER must be 3, 5 or 7");
+        static_assert(ORDER == 7, "ORDER must be 3, 5, 7 or 9");
         vL = R((-RR(3.0) * s[0] + RR(25.0) * s[1] - RR(101.0) * s[2] + RR(319.0) * s[3]
                 + RR(214.0) * s[4] - RR(38.0) * s[5] + RR(4.0) * s[6]) / RR(420.0));
         vR = R((RR(4.0) * s[1] - RR(38.0) * s[2] + RR(214.0) * s[3] + RR(319.0) * s[4]
@@ -259,6 +266,15 @@ __device__ __forceinline__ void upface_fast(const R *s, R &vL, R &vR)
         const R k = R(1.0 / 60.0);
         vL = (R(2) * s[0] - R(13) * s[1] + R(47) * s[2] + R(27) * s[3] - R(3) * s[4]) * k;
         vR = (-R(3) * s[1] + R(27) * s[2] + R(47) * s[3] - R(13) * s[4] + R(2) * s[5]) * k;
+    } else if constexpr (ORDER == 9) {
+#define FVB_W9(a) R((a) / 2520.0)
+        vL = FVB_W9(3.) * s[0] + FVB_W9(-25.) * s[1] + FVB_W9(101.) * s[2] + FVB_W9(-319.) * s[3]
+             + FVB_W9(2765.) * s[4] + FVB_W9(2139.) * s[5] + FVB_W9(-533.) * s[6] + FVB_W9(97.) * s[7]
+             + FVB_W9(-11.) * s[8];
+        vR = FVB_W9(-11.) * s[1] + FVB_W9(97.) * s[2] + FVB_W9(-533.) * s[3] + FVB_W9(2139.) * s[4]
+             + FVB_W9(2765.) * s[5] + FVB_W9(-319.) * s[6] + FVB_W9(101.) * s[7] + FVB_W9(-25.) * s[8]
+             + FVB_W9(3.) * s[9];
+#undef FVB_W9
     } else {
         // weights pre-divided: one multiply and six fused multiply-adds a side
 #define FVB_W7(a) R((a) / 420.0)

@@ -462,9 +462,11 @@ static KernelEntry *table_for(int prec, int order, int rs = 0)
     static KernelEntry t64_7[] = {FVB_SHAPES(P64, 7)};
     static KernelEntry t64_5[] = {FVB_SHAPES(P64, 5)};
     static KernelEntry t64_3[] = {FVB_SHAPES(P64, 3)};
+    static KernelEntry t64_9[] = {FVB_SHAPES(P64, 9)};
     static KernelEntry t32_7[] = {FVB_SHAPES(P32, 7)};
     static KernelEntry t32c_7[] = {entry32c(0), entry32c(1), entry32c(2), entry32c(3), entry32c(4), entry32c(5)};
-    if (prec == P64) return order == 7 ? t64_7 : order == 5 ? t64_5 : order == 3 ? t64_3 : nullptr;
+    if (prec == P64)
+        return order == 7 ? t64_7 : order == 5 ? t64_5 : order == 3 ? t64_3 : order == 9 ? t64_9 : nullptr;
     if (order != 7) return nullptr;
     return prec == P32 ? t32_7 : prec == P32C ? t32c_7 : nullptr;
 }

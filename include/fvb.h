@@ -56,7 +56,7 @@ typedef enum fvb_flux {
     /* the scheme kept in fv_up7_ducros_2d.cu.bak: UP-order reconstruction of
      * the conserved variables, HLLC, and a D2 artificial viscosity gated by
      * a Ducros weight from the 6th-order velocity divergence
-     * (fv_up7_ducros_2d.cu.bak:287-390; FP64, order 3, 5 or 7, ghost width
+     * (fv_up7_ducros_2d.cu.bak:287-390; FP64, order 3, 5, 7 or 9, ghost width
      * max((order + 1) / 2, 3); coefficients from fvb_set_d2av) */
     FVB_FLUX_UP_HLLC_D2AV = 5
 } fvb_flux;
@@ -101,7 +101,7 @@ typedef enum fvb_case_kind {
 /* One grid: N x N cells on [x0, x0 + length] x [y0, y0 + length], h = length / N. */
 typedef struct fvb_config {
     int n;                    /* cells per side (>= g)                            */
-    int order;                /* UP order: 3, 5 or 7 (ignored by KEEP)            */
+    int order;                /* UP order: 3, 5, 7 or 9 (ignored by KEEP)         */
     int flux;                 /* fvb_flux                                         */
     int precision;            /* fvb_precision                                    */
     int bc_x, bc_y;           /* fvb_bc on the x and y boundaries                 */

@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 FREESTREAM = [
     ("up_ducros", "f64", 7), ("up_ducros", "f64", 3), ("up_ducros", "f32", 7), ("up_ducros", "f32c", 7),
     ("up_ducros_hll", "f64", 7), ("up_ducros_roe", "f64", 7), ("keep", "f64", 7), ("rec3", "f64", 7),
-    ("up_hllc_d2av", "f64", 5),
+    ("up_hllc_d2av", "f64", 5), ("up_ducros", "f64", 9), ("up_hllc_d2av", "f64", 9),
 ]
 
 

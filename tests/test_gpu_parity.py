@@ -56,6 +56,24 @@ def test_up_rhs_matches_oracle(n, dtype, tol):
     assert rel_linf(lam.cpu().numpy()[None], l[None]) <= tol
 
 
+@pytest.mark.parametrize("order", [3, 5, 9])
+@pytest.mark.parametrize("n", [9, 40])
+def test_up_rhs_orders_match_oracle(order, n):
+    """The other UP orders of fv_up7_ducros_2d.cu:149-186 (FP64), UP9 with
+    its published weights."""
+    g = (order + 1) // 2
+    U = _padded(smooth(n, seed=n), 0, g)
+    h = 1.0 / n
+    Qd = torch.from_numpy(U).cuda()
+    rhs = torch.empty((4, n, n), dtype=Qd.dtype, device="cuda")
+    lam = torch.empty((n, n), dtype=Qd.dtype, device="cuda")
+    F.up_rhs(Qd, rhs, lam, n, n + 2 * g, h, order=order)
+    torch.cuda.synchronize()
+    R, l = O.up_rhs(U, n, h, order=order)
+    assert rel_linf(rhs.cpu().numpy(), R) <= 1e-13
+    assert rel_linf(lam.cpu().numpy()[None], l[None]) <= 1e-13
+
+
 @pytest.mark.skipif(not O.have_ref_gpu(), reason="reference GPU build absent")
 @pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-13), (np.float32, 2e-5)])
 def test_up_rhs_matches_reference_kernel(dtype, tol):
@@ -135,27 +153,49 @@ def test_step_f64_matches_oracle(bc, n, case):
         # edge; floored reconstructions there make any two builds differ at
         # ~1e-11 (the same conditioning the sharp-jump cases showed)
         pytest.skip("periodic wrap of a four-quadrant state is not smooth")
+    _step_against_oracle(bc, n, case, 7)
+
+
+def _step_against_oracle(bc, n, case, order):
+    g = (order + 1) // 2
     w = CASES[case](n)
     length = 10.0 if case == "vortex" else 1.0
-    U = _padded(w, BCS[bc])
-    s = F.Solver(n, bc=bc, length=length, x0=-5.0 if case == "vortex" else 0.0,
+    U = _padded(w, BCS[bc], g)
+    s = F.Solver(n, order=order, bc=bc, length=length, x0=-5.0 if case == "vortex" else 0.0,
                  y0=-5.0 if case == "vortex" else 0.0, cfl=0.45)
     s.set_state(U)
-    steps = 12
+    # UP9's published weights scale every reconstructed state by 4217/2520,
+    # and the scheme doubles a perturbation about every step: on the 37^2
+    # vortex the oracle against itself with a 1-ulp change of the initial
+    # state differs by 1.7e-14 after 3 steps, 5.1e-13 after 6 and 7.3e-12
+    # after 12 (UP7: 1.9e-15 after 12), so UP9 is compared after 4 steps
+    steps = 4 if order == 9 else 12
     s.step(steps)
     st = s.sync()
     got = s.get_state()
     ref = U.copy()
-    status, t, k, lmax, dt = O.up_run(ref, n, length / n, 0.45, BCS[bc], steps)
+    status, t, k, lmax, dt = O.up_run(ref, n, length / n, 0.45, BCS[bc], steps, order=order)
     # the same stop, at the same step, when the scheme itself breaks down
     assert st.status == {0: 0, 1: F._lib.ERR_BLOWUP, 2: F._lib.ERR_DT_UNDERFLOW}[status]
     assert st.steps == k
     if status:
         return
+    err = rel_linf(_cons(got, g), _cons(ref, g))
+    print("UP%d %s %s %d^2 x %d: rel L-inf %.2e, t rel %.2e" % (order, case, bc, n, steps, err, abs(st.t - t) / t))
     assert abs(st.t - t) <= 1e-13 * t
-    assert rel_linf(_cons(got), _cons(ref)) <= TOL64
+    assert err <= TOL64
     # the ghost ring is the boundary rule applied to the new interior
     assert rel_linf(got, ref) <= TOL64
+
+
+@pytest.mark.parametrize("order", [3, 5, 9])
+@pytest.mark.parametrize("bc", ["reflect", "periodic", "transmissive"])
+@pytest.mark.parametrize("n,case", [(17, "smooth"), (37, "vortex"), (40, "sod")])
+def test_orders_step_f64_matches_oracle(order, bc, n, case):
+    """Whole steps at the other UP orders (FP64; the reference selects the
+    order with its ORDER macro, fv_up7_ducros_2d.cu:30-37), UP9 with its
+    published weights."""
+    _step_against_oracle(bc, n, case, order)
 
 
 @pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
