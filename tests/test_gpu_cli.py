@@ -70,6 +70,28 @@ def test_fvb_up7_d2av_frames(tmp_path):
     assert np.array_equal(c.get_state(layout="cons", interior=True), want)
 
 
+@pytest.mark.parametrize("args,order,flux", [(["--order", "9"], 9, "up_ducros"),
+                                               (["--d2av", "40", "0.5", "0", "0.05", "9"], 9, "up_hllc_d2av")])
+def test_fvb_up7_order9(tmp_path, args, order, flux):
+    """UP9 from the command line: fv_up7 built with ORDER 9, and the .bak's
+    fifth argument 9; the state at the end equals a library run"""
+    if args[0] == "--order":
+        args = ["40"] + args
+    r = subprocess.run([str(BIN / "fvb_up7"), *args, "--t-end", "0.01", "--frames", "1", "--save", "end.ckpt"],
+                       cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert "order=9" in r.stdout and "UP9" in r.stdout
+    s = F.Solver(40, order=order, flux=flux)
+    if flux == "up_hllc_d2av":
+        s.init_case("sod", rho_in=10.0)
+    else:
+        s.init_case("sod")
+    s.advance(0.01)
+    c = F.Solver(40, order=order, flux=flux)
+    c.load(str(tmp_path / "end.ckpt"))
+    assert np.array_equal(c.get_state(layout="cons", interior=True), s.get_state(layout="cons", interior=True))
+
+
 def test_fvb_up7_frames(tmp_path):
     r = subprocess.run([str(BIN / "fvb_up7"), "48", "--t-end", "0.02", "--frames", "2", "--bin"], cwd=tmp_path,
                        capture_output=True, text=True, timeout=120)
