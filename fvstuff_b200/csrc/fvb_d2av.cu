@@ -341,19 +341,11 @@ int sm_count()
 template <int ORDER>
 cudaError_t launch_order(const GridDev &gd, int stage, int tiles, const D2Params &av, cudaStream_t s)
 {
-    static bool ready = false;
-    static int ctas_per_sm = 0;
     constexpr size_t smem = D2Shape<ORDER>::SMEM;
-    if (!ready) {
-        cudaError_t e =
-            cudaFuncSetAttribute(d2av_stage_kernel<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, d2av_stage_kernel<ORDER>, DNT, smem);
-        if (e != cudaSuccess) return e;
-        if (ctas_per_sm <= 0) return cudaErrorInvalidConfiguration;
-        ready = true;
-    }
-    const int cap = ctas_per_sm * sm_count();
+    LaunchFacts f{};
+    cudaError_t e = launch_facts((const void *)d2av_stage_kernel<ORDER>, DNT, smem, f);
+    if (e != cudaSuccess) return e;
+    const int cap = f.ctas_per_sm * f.sms;
     d2av_stage_kernel<ORDER><<<tiles < cap ? tiles : cap, DNT, smem, s>>>(gd, stage, tiles, av);
     return cudaGetLastError();
 }

@@ -120,4 +120,16 @@ cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int
 size_t stage_smem_bytes(int prec, int order, int shape, int rs = 0);
 int stage_max_ctas_per_sm(int prec, int order, int shape, int rs = 0);
 
+// What a persistent launch of kernel `fn` with `threads` threads and `smem`
+// bytes of dynamic shared memory needs on the current device: the shared-
+// memory opt-in is applied and the resident CTAs per SM and the SM count
+// are read once per (kernel, device, threads, smem), under a lock, so
+// solvers on several host threads or devices set it up safely
+// (fvb_stage.cu).  An error if not even one CTA fits on an SM.
+struct LaunchFacts {
+    int ctas_per_sm;
+    int sms;
+};
+cudaError_t launch_facts(const void *fn, int threads, size_t smem, LaunchFacts &out);
+
 }  // namespace fvb

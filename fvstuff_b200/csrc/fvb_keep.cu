@@ -332,21 +332,12 @@ void keep_tiles(int n, int &tiles_x, int &tiles)
 // fused flux / RK / ghost kernel
 cudaError_t keep_launch_stage(const GridDev &gd, int stage, int tiles, cudaStream_t s)
 {
-    static bool ready = false;
-    static int ctas_per_sm = 0, sms = 0;
-    if (!ready) {
-        cudaError_t e = cudaFuncSetAttribute(keep_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)keep_smem());
-        if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, keep_stage_kernel, KNT, keep_smem());
-        if (e != cudaSuccess) return e;
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        ready = true;
-    }
+    LaunchFacts f{};
+    cudaError_t e = launch_facts((const void *)keep_stage_kernel, KNT, keep_smem(), f);
+    if (e != cudaSuccess) return e;
+    const int ctas_per_sm = f.ctas_per_sm, sms = f.sms;
     const void *in = stage == 2 ? gd.k1 : stage == 3 ? gd.k2 : gd.st[0];
-    cudaError_t e = cudaMemsetAsync(&gd.ctrl->aux, 0, sizeof(unsigned long long), s);
+    e = cudaMemsetAsync(&gd.ctrl->aux, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
     const int eb = tiles < 4 * sms ? tiles : 4 * sms;
     keep_ed_kernel<<<eb, KNT, 0, s>>>(gd, (const double *)in, tiles);

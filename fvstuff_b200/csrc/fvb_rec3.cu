@@ -424,17 +424,10 @@ void rec3_tiles(int n, int &tiles_x, int &tiles)
 
 cudaError_t rec3_launch_stage(const GridDev &gd, int stage, int tiles, cudaStream_t s)
 {
-    static bool ready = false;
-    static int ctas_per_sm = 0;
-    if (!ready) {
-        cudaError_t e = cudaFuncSetAttribute(rec3_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)rec3_smem());
-        if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, rec3_stage_kernel, RNT, rec3_smem());
-        if (e != cudaSuccess) return e;
-        ready = true;
-    }
-    const int cap = ctas_per_sm * sm_count();
+    LaunchFacts f{};
+    cudaError_t e = launch_facts((const void *)rec3_stage_kernel, RNT, rec3_smem(), f);
+    if (e != cudaSuccess) return e;
+    const int cap = f.ctas_per_sm * f.sms;
     rec3_stage_kernel<<<tiles < cap ? tiles : cap, RNT, rec3_smem(), s>>>(gd, stage, tiles);
     return cudaGetLastError();
 }

@@ -21,6 +21,9 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "fvb_internal.h"
 #include "fvb_physics.cuh"
@@ -431,21 +434,19 @@ struct KernelEntry {
     void *fn_batched;  // tile table
     size_t smem;
     int nt;
-    int ready;
-    int max_ctas;
 };
 
 template <int PREC, int ORDER, int SHAPE, int RS = 0>
 static KernelEntry entry()
 {
     using KK = K<PREC, ORDER, SHAPE, RS>;
-    return KernelEntry{KK::fn(), KK::fn_batched(), KK::smem(), kTileShapes[SHAPE].nt, 0, 0};
+    return KernelEntry{KK::fn(), KK::fn_batched(), KK::smem(), kTileShapes[SHAPE].nt};
 }
 
 static KernelEntry entry32c(int shape)
 {
     return KernelEntry{stage32c_fn(shape, false), stage32c_fn(shape, true), stage32c_smem(shape),
-                       kTileShapes[shape].nt, 0, 0};
+                       kTileShapes[shape].nt};
 }
 
 #define FVB_SHAPES(P, O) \
@@ -471,20 +472,39 @@ static KernelEntry *table_for(int prec, int order, int rs = 0)
     return prec == P32 ? t32_7 : prec == P32C ? t32c_7 : nullptr;
 }
 
-static cudaError_t prepare(KernelEntry &e)
+cudaError_t launch_facts(const void *fn, int threads, size_t smem, LaunchFacts &out)
 {
-    if (e.ready) return cudaSuccess;
-    int nb = 1 << 30;
-    for (void *f : {e.fn, e.fn_batched}) {
-        cudaError_t err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem);
-        if (err != cudaSuccess) return err;
-        int k = 0;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, f, e.nt, e.smem);
-        if (err != cudaSuccess) return err;
-        nb = std::min(nb, k);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::map<std::tuple<const void *, int, int, size_t>, LaunchFacts> known;
+    const auto key = std::make_tuple(fn, dev, threads, smem);
+    std::lock_guard<std::mutex> lk(mu);
+    const auto it = known.find(key);
+    if (it != known.end()) {
+        out = it->second;
+        return cudaSuccess;
     }
-    e.max_ctas = nb;
-    e.ready = 1;
+    LaunchFacts f{};
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f.ctas_per_sm, fn, threads, smem);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&f.sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    if (f.ctas_per_sm <= 0) return cudaErrorInvalidConfiguration;
+    known.emplace(key, f);
+    out = f;
+    return cudaSuccess;
+}
+
+// resident CTAs per SM of a table entry: the fewer of its two kernels
+static cudaError_t prepare(const KernelEntry &e, int &max_ctas)
+{
+    LaunchFacts a{}, b{};
+    cudaError_t err = launch_facts(e.fn, e.nt, e.smem, a);
+    if (err == cudaSuccess) err = launch_facts(e.fn_batched, e.nt, e.smem, b);
+    if (err != cudaSuccess) return err;
+    max_ctas = std::min(a.ctas_per_sm, b.ctas_per_sm);
     return cudaSuccess;
 }
 
@@ -571,16 +591,18 @@ int stage_max_ctas_per_sm(int prec, int order, int shape, int rs)
 {
     KernelEntry *t = table_for(prec, order, rs);
     if (!t || shape < 0 || shape >= kNumTileShapes) return 0;
-    if (prepare(t[shape]) != cudaSuccess) return 0;
-    return t[shape].max_ctas;
+    int max_ctas = 0;
+    if (prepare(t[shape], max_ctas) != cudaSuccess) return 0;
+    return max_ctas;
 }
 
 cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int grid_ctas, cudaStream_t s, int rs)
 {
     KernelEntry *t = table_for(prec, order, rs);
     if (!t || shape < 0 || shape >= kNumTileShapes) return cudaErrorInvalidValue;
-    KernelEntry &e = t[shape];
-    cudaError_t err = prepare(e);
+    const KernelEntry &e = t[shape];
+    int max_ctas = 0;
+    cudaError_t err = prepare(e, max_ctas);
     if (err != cudaSuccess) return err;
     if (grid_ctas <= 0) return cudaSuccess;
     void *args[] = {(void *)&a};

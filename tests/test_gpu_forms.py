@@ -217,3 +217,42 @@ def test_serve_stream_matches_alone():
         assert abs(r["t"] - d.t_end) <= 1e-12
     lat = sorted(r["finished"] - r["arrival"] for r in res)
     print("serve: %d requests in %.3f s, p50 %.4f s p99 %.4f s" % (len(res), wall, lat[len(lat) // 2], lat[-1]))
+
+
+def test_solvers_on_concurrent_host_threads():
+    """One solver per host thread (the C ABI's threading rule): solvers of
+    every kernel family, created and stepped on four threads at once -- each
+    setting up its kernels for the first time -- give the results they give
+    one after another."""
+    import threading
+
+    specs = [dict(flux="up_ducros", precision="f64", order=9), dict(flux="keep"),
+             dict(flux="rec3", bc="periodic"), dict(flux="up_hllc_d2av", order=9)]
+
+    def run(spec):
+        kw = dict(spec)
+        kw.setdefault("bc", "reflect")
+        s = F.Solver(48, **kw)
+        s.init_case("sod")
+        s.step(10)
+        s.sync()
+        out = s.get_state(interior=True)
+        s.close()
+        return out
+
+    got, errors = [None] * len(specs), []
+
+    def worker(k):
+        try:
+            got[k] = run(specs[k])
+        except Exception as e:  # reported below, on the main thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(len(specs))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for k, spec in enumerate(specs):
+        assert np.array_equal(got[k], run(spec), equal_nan=True), spec
