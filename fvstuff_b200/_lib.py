@@ -52,7 +52,8 @@ class InstanceDesc(C.Structure):
 
 
 class Request(C.Structure):
-    _fields_ = [("arrival", C.c_double), ("desc", InstanceDesc)]
+    _fields_ = [("arrival", C.c_double), ("desc", InstanceDesc), ("out", C.c_void_p), ("out_layout", C.c_int),
+                ("out_dtype", C.c_int)]
 
 
 class RequestResult(C.Structure):
@@ -61,8 +62,11 @@ class RequestResult(C.Structure):
 
 
 class ServeConfig(C.Structure):
-    _fields_ = [("batch", BatchConfig), ("steps_per_round", C.c_int), ("keep_results", C.c_int),
+    _fields_ = [("batch", BatchConfig), ("steps_per_round", C.c_int), ("policy", C.c_int), ("max_cells", C.c_double),
                 ("max_seconds", C.c_double)]
+
+
+SERVE_POLICY = {"fifo": 0, "shortest": 1}
 
 
 _P = C.c_void_p

@@ -83,21 +83,37 @@ class Batch:
 
 
 def serve_run(requests, precision: str = "f32c", hbm_budget: int = 0, steps_per_round: int = 8,
-              max_instances: int = 0, max_seconds: float = 0.0, device: int = 0):
+              max_instances: int = 0, max_seconds: float = 0.0, device: int = 0, policy: str = "fifo",
+              max_cells: float = 0.0, keep_results: bool = False, layout: str = "prim", dtype=np.float64):
     """Play a list of (arrival_seconds, InstanceDesc) through fvb_serve_run;
-    returns (results as a list of dicts, wall seconds)."""
+    returns (results as a list of dicts, wall seconds).  `policy` "fifo"
+    admits in arrival order, "shortest" least estimated work (n^3 t_end)
+    first; `max_cells` caps the interior cells of the live instances (0: HBM
+    budget and slots only).  With `keep_results` each result carries the
+    final interior state ("state", 4 x n x n in `layout` / `dtype`)."""
     n = len(requests)
     reqs = (L.Request * n)()
+    states = []
     for i, (t, d) in enumerate(requests):
         reqs[i].arrival = t
         reqs[i].desc = d
+        if keep_results:
+            a = np.empty((4, d.n, d.n), dtype)
+            states.append(a)
+            reqs[i].out = a.ctypes.data
+            reqs[i].out_layout = LAYOUT[layout]
+            reqs[i].out_dtype = 1 if a.dtype == np.float64 else 0
     res = (L.RequestResult * n)()
     cfg = L.ServeConfig()
     cfg.batch.precision, cfg.batch.order, cfg.batch.device = PREC[precision], 7, device
     cfg.batch.hbm_budget, cfg.batch.max_instances, cfg.batch.use_graph, cfg.batch.tile = hbm_budget, max_instances, 1, -1
     cfg.steps_per_round, cfg.max_seconds = steps_per_round, max_seconds
+    cfg.policy, cfg.max_cells = L.SERVE_POLICY[policy], float(max_cells)
     wall = C.c_double()
     check(lib().fvb_serve_run(C.byref(cfg), reqs, n, res, C.byref(wall)), "fvb_serve_run")
     out = [dict(arrival=requests[i][0], admitted=r.admitted, finished=r.finished, status=r.status,
                 steps=int(r.steps), t=r.t) for i, r in enumerate(res)]
+    if keep_results:
+        for o, a in zip(out, states):
+            o["state"] = a
     return out, wall.value

@@ -1,12 +1,13 @@
 // fvb_serve.cpp -- serving loop over the batched form (continuous batching).
 //
 // Requests become visible at their arrival time.  Between batch rounds the
-// loop admits waiting requests in arrival order while the HBM budget and
-// the instance slots allow, advances every admitted instance together for
-// `steps_per_round` steps (one persistent launch per RK stage, graph
-// replayed), then retires the instances that reached their t_end and frees
-// their memory, so later arrivals join as room appears.  States never leave
-// the device unless `keep_results` asks for a copy.
+// loop admits waiting requests -- in arrival order, or least estimated work
+// first -- while the HBM budget, the instance slots and the cell cap allow,
+// advances every admitted instance together for `steps_per_round` steps
+// (one persistent launch per RK stage, graph replayed), then retires the
+// instances that reached their t_end and frees their memory, so later
+// arrivals join as room appears.  States never leave the device except the
+// final state a request asks for (copied out as it retires).
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -38,6 +39,10 @@ extern "C" fvb_status fvb_serve_run(const fvb_serve_config *cfg, const fvb_reque
     }
     std::vector<int> slot_req(65536, -1);
     std::deque<int> waiting;
+    // the shortest-first key: cells x steps, steps ~ n t_end at a fixed CFL
+    auto work = [&](int r) { const double n = reqs[r].desc.n; return n * n * n * reqs[r].desc.t_end; };
+    const bool shortest = cfg->policy == FVB_SERVE_SHORTEST_FIRST;
+    double live_cells = 0.0;
     size_t next = 0;
     int done = 0;
     const auto t0 = clk::now();
@@ -46,11 +51,19 @@ extern "C" fvb_status fvb_serve_run(const fvb_serve_config *cfg, const fvb_reque
     fvb_status result = FVB_OK;
     while (done < nreq) {
         double tnow = now();
-        while (next < order.size() && reqs[order[next]].arrival <= tnow) waiting.push_back(order[next++]);
-        // admission in arrival order; a request that does not fit waits
+        bool arrived = false;
+        while (next < order.size() && reqs[order[next]].arrival <= tnow) {
+            waiting.push_back(order[next++]);
+            arrived = true;
+        }
+        if (shortest && arrived)
+            std::stable_sort(waiting.begin(), waiting.end(), [&](int x, int y) { return work(x) < work(y); });
+        // admission in the policy's order; a request that does not fit waits
         // (head of line) until an instance retires
         while (!waiting.empty()) {
             int r = waiting.front();
+            const double cells = (double)reqs[r].desc.n * reqs[r].desc.n;
+            if (cfg->max_cells > 0 && live_cells > 0 && live_cells + cells > cfg->max_cells) break;
             int id = -1;
             fvb_status a = fvb_batch_add(b, &reqs[r].desc, &id);
             if (a == FVB_ERR_NOMEM) {
@@ -72,6 +85,7 @@ extern "C" fvb_status fvb_serve_run(const fvb_serve_config *cfg, const fvb_reque
             }
             slot_req[id] = r;
             res[r].admitted = now();
+            live_cells += cells;
             waiting.pop_front();
         }
         if (fvb_batch_active(b) == 0) {
@@ -96,11 +110,19 @@ extern "C" fvb_status fvb_serve_run(const fvb_serve_config *cfg, const fvb_reque
                 res[r].steps = s.steps;
                 res[r].t = s.t;
             }
+            if (reqs[r].out) {
+                const fvb_status g =
+                    fvb_batch_get_state(b, id, reqs[r].out, reqs[r].out_layout, reqs[r].out_dtype, 1);
+                if (g) { result = g; break; }
+                tf = now();
+            }
             res[r].finished = tf;
             slot_req[id] = -1;
+            live_cells -= (double)reqs[r].desc.n * reqs[r].desc.n;
             fvb_batch_remove(b, id);
             ++done;
         }
+        if (result) break;
         if (cfg->max_seconds > 0 && now() > cfg->max_seconds) { result = fail(FVB_ERR_TIMEOUT, "serving run exceeded %.1f s", cfg->max_seconds); break; }
     }
     if (wall_seconds) *wall_seconds = now();

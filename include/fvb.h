@@ -304,6 +304,11 @@ FVB_API size_t fvb_batch_bytes_in_use(const fvb_batch *b);
 typedef struct fvb_request {
     double arrival;           /* seconds after the start of the run                */
     fvb_instance_desc desc;
+    void *out;                /* host buffer for the final interior state (4 x n x n
+                               * in out_layout / out_dtype), written before the
+                               * instance retires; NULL = keep no result          */
+    int out_layout;           /* FVB_LAYOUT_PRIM or FVB_LAYOUT_CONS                */
+    int out_dtype;            /* FVB_F64 or FVB_F32                                */
 } fvb_request;
 
 typedef struct fvb_request_result {
@@ -314,17 +319,28 @@ typedef struct fvb_request_result {
     double t;
 } fvb_request_result;
 
+enum {
+    FVB_SERVE_FIFO = 0,           /* admit in arrival order                          */
+    FVB_SERVE_SHORTEST_FIRST = 1  /* admit the waiting request of least estimated
+                                   * work first (n^3 t_end: cells x steps)           */
+};
+
 typedef struct fvb_serve_config {
     fvb_batch_config batch;
     int steps_per_round;      /* steps per batch round between admissions (0 = 8) */
-    int keep_results;         /* copy each final state to host memory (slower)     */
+    int policy;               /* FVB_SERVE_FIFO or FVB_SERVE_SHORTEST_FIRST        */
+    double max_cells;         /* admit while the live instances hold fewer interior
+                               * cells than this (0 = no limit but HBM and slots);
+                               * one instance is always admitted                   */
     double max_seconds;       /* give up after this long (0 = no limit)            */
 } fvb_serve_config;
 
 /* Play the request stream in real time: requests become visible at their
- * arrival time, are admitted as HBM budget and slots free up, advance
- * together, and are retired when they reach t_end.  Blocks until all are
- * done.  res[i] matches reqs[i]. */
+ * arrival time, are admitted (in the policy's order; a request that does not
+ * fit blocks the ones behind it) as HBM budget, slots and the cell cap allow,
+ * advance together, and are retired when they reach t_end, their final state
+ * copied to reqs[i].out first.  Blocks until all are done.  res[i] matches
+ * reqs[i]. */
 FVB_API fvb_status fvb_serve_run(const fvb_serve_config *cfg, const fvb_request *reqs, int nreq,
                          fvb_request_result *res, double *wall_seconds);
 

@@ -34,6 +34,32 @@ def test_library_exports_every_declared_symbol():
         assert getattr(lib, name) is not None
 
 
+STRUCTS = {"fvb_config": L.Config, "fvb_case": L.Case, "fvb_stats": L.Stats, "fvb_batch_config": L.BatchConfig,
+           "fvb_instance_desc": L.InstanceDesc, "fvb_request": L.Request, "fvb_request_result": L.RequestResult,
+           "fvb_serve_config": L.ServeConfig}
+
+
+def test_struct_layouts_match_bindings(tmp_path):
+    """Every struct of the header has the size and field offsets the ctypes
+    mirror gives it (compiled here with the system C compiler)."""
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "fvb.h"', "int main(void) {"]
+    for cname, cls in STRUCTS.items():
+        lines.append('printf("%s %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f in cls._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (cname, f[0], cname, f[0]))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), "-o", str(exe), str(src)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                        check=True).stdout.splitlines())
+    for cname, cls in STRUCTS.items():
+        assert int(got[cname]) == C.sizeof(cls), cname
+        for f in cls._fields_:
+            assert int(got[cname + "." + f[0]]) == getattr(cls, f[0]).offset, (cname, f[0])
+
+
 def test_version_and_defaults():
     assert F.lib().fvb_version().startswith(b"fvb")
     cfg = L.Config()

@@ -201,22 +201,43 @@ def test_batch_bad_instances_stay_isolated(prec):
 
 # --- serving loop ---------------------------------------------------------------
 
-def test_serve_stream_matches_alone():
+@pytest.mark.parametrize("policy,max_cells", [("fifo", 0), ("shortest", 12000)])
+def test_serve_stream_matches_alone(policy, max_cells):
+    """Every request of a stream finishes at its t_end with the state the
+    same grid reaches alone, bit for bit, whatever joined it on the device;
+    with a cell cap the live instances never hold more than the cap (but
+    one)."""
     rng = np.random.default_rng(0)
-    reqs = []
+    reqs, cases = [], []
     t = 0.0
     for k in range(12):
         t += rng.exponential(1 / 200.0)
         n = int(rng.choice([32, 48, 64, 80]))
-        d, _ = _desc(n, 500 + k, float(rng.uniform(0.02, 0.06)))
+        d, c = _desc(n, 500 + k, float(rng.uniform(0.02, 0.06)))
         reqs.append((t, d))
-    res, wall = F.serve_run(reqs, precision="f32c", steps_per_round=4)
+        cases.append(c)
+    res, wall = F.serve_run(reqs, precision="f32c", steps_per_round=4, policy=policy, max_cells=max_cells,
+                            keep_results=True)
     assert all(r["status"] == 0 and r["finished"] >= r["admitted"] >= 0 for r in res)
-    for (arr, d), r in zip(reqs, res):
+    for (arr, d), r, c in zip(reqs, res, cases):
         assert r["admitted"] >= arr - 1e-3
         assert abs(r["t"] - d.t_end) <= 1e-12
+        s = F.Solver(d.n, precision="f32c", bc="transmissive", cfl=0.5)
+        s.init_case(c)
+        s.advance(d.t_end)
+        assert s.sync().steps == r["steps"]
+        assert np.array_equal(r["state"], s.get_state(interior=True))
+        s.close()
+    if max_cells:
+        # at every admission the cells already live plus the newcomer's fit
+        # the cap, unless nothing else was live
+        for i, (_, d) in enumerate(reqs):
+            live = sum(reqs[j][1].n ** 2 for j, o in enumerate(res)
+                       if j != i and o["admitted"] <= res[i]["admitted"] < o["finished"])
+            assert live == 0 or live + d.n ** 2 <= max_cells, (i, live)
     lat = sorted(r["finished"] - r["arrival"] for r in res)
-    print("serve: %d requests in %.3f s, p50 %.4f s p99 %.4f s" % (len(res), wall, lat[len(lat) // 2], lat[-1]))
+    print("serve %s: %d requests in %.3f s, p50 %.4f s p99 %.4f s" % (policy, len(res), wall, lat[len(lat) // 2],
+                                                                        lat[-1]))
 
 
 def test_solvers_on_concurrent_host_threads():
