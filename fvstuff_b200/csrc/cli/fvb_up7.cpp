@@ -5,6 +5,7 @@
 //           [--gamma G] [--bc reflect|periodic|transmissive] [--order 3|5|7|9]
 //           [--precision f64|f32|f32c] [--frames F] [--prefix P] [--seed S]
 //           [--bin] [--no-ppm] [--save FILE] [--resume FILE]
+//           [--metrics FILE] (JSON lines: per frame, blow-up and the end)
 //   fvb_up7 --d2av [N [C2 [Cg [sc [order]]]]] [options above]
 //
 // Defaults are the reference's: N = 400, CFL 0.40, t_end 1, circular Sod
@@ -34,7 +35,7 @@ struct Args {
     int n = 400, order = 7, frames = 10, precision = FVB_PREC_F64, bc = -1, kase = FVB_CASE_SOD;
     double cfl = 0.40, t_end = 1.0, gamma = 1.4;
     long long seed = -1;
-    std::string prefix = "sod", save, resume;
+    std::string prefix = "sod", save, resume, metrics;
     bool bin = false, ppm = true;
     bool d2av = false;
     double c2 = 0.5, cg = 0.0, sc = 0.05;
@@ -77,6 +78,7 @@ Args parse(int argc, char **argv)
         else if (s == "--no-ppm") a.ppm = false;
         else if (s == "--save") a.save = val();
         else if (s == "--resume") a.resume = val();
+        else if (s == "--metrics") a.metrics = val();
         else if (s == "--d2av") continue;
         else if (s[0] != '-' && !a.d2av) a.n = std::atoi(s.c_str());
         else if (s[0] != '-') {
@@ -206,6 +208,25 @@ int main(int argc, char **argv)
     const auto t0 = std::chrono::steady_clock::now();
     auto elapsed = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
     long long last_print = st.steps;
+    // JSON-lines metrics: one line per frame, blow-up and the end, with the
+    // throughput since the start of the loop and the HBM traffic it implies
+    // (85.33 B per cell-stage with 8-byte or hi/lo words, 42.67 B in FP32)
+    std::FILE *mf = a.metrics.empty() ? nullptr : std::fopen(a.metrics.c_str(), "w");
+    if (!a.metrics.empty() && !mf) { std::fprintf(stderr, "cannot write %s\n", a.metrics.c_str()); return 1; }
+    const long long steps0 = st.steps;
+    const double bytes_cs = a.precision == FVB_PREC_F32 ? 128.0 / 3.0 : 256.0 / 3.0;
+    auto metric = [&](const char *event, const fvb_stats &cur) {
+        if (!mf) return;
+        const double wall = elapsed(), cs = 3.0 * a.n * (double)a.n * (double)(cur.steps - steps0);
+        const double rate = wall > 0 ? cs / wall : 0.0;
+        std::fprintf(mf,
+                     "{\"event\": \"%s\", \"n\": %d, \"order\": %d, \"precision\": \"%s\", \"step\": %lld, "
+                     "\"t\": %.17g, \"dt\": %.17g, \"lam_max\": %.17g, \"wall_s\": %.6f, "
+                     "\"cell_stage_per_s\": %.6g, \"hbm_gbs\": %.6g}\n",
+                     event, a.n, a.order, a.precision == FVB_PREC_F64 ? "f64" : a.precision == FVB_PREC_F32 ? "f32" : "f32c",
+                     (long long)cur.steps, cur.t, cur.dt, cur.lam_max, wall, rate, rate * bytes_cs / 1e9);
+        std::fflush(mf);
+    };
     bool enqueued = false;  // steps already on the stream (issued behind a frame)
     // at most 50 steps per call so progress prints like the reference's
     auto issue = [&](const fvb_stats &cur) {
@@ -221,12 +242,14 @@ int main(int argc, char **argv)
                          st.status == FVB_ERR_BLOWUP ? "NaN/Inf lam_max" : "dt underflow", (long long)st.steps, st.t,
                          st.lam_max);
             write_frame_now(s, F, a, 99);
+            metric(st.status == FVB_ERR_BLOWUP ? "blowup" : "dt_underflow", st);
             break;
         }
         if (st.t >= t_next - 1e-12 && frame <= a.frames) {
             std::printf("  frame %2d/%d  step %5lld  t=%.5f  elapsed=%.1fs\n", frame, a.frames, (long long)st.steps,
                         st.t, elapsed());
             std::fflush(stdout);
+            metric("frame", st);
             if (fvb_frame_begin(s)) { std::fprintf(stderr, "frame: %s\n", fvb_last_error()); return 1; }
             ++frame;
             t_next = frame * a.t_end / a.frames;
@@ -245,6 +268,8 @@ int main(int argc, char **argv)
         last_print = st.steps;
     }
     std::printf("  Done: %lld steps,  t=%.6f,  wall=%.2fs\n", (long long)st.steps, st.t, elapsed());
+    metric("done", st);
+    if (mf) std::fclose(mf);
     if (a.ppm) std::printf("  Frames written: %s_0000.ppm .. %s_%04d.ppm  (2x2 composite)\n", a.prefix.c_str(), a.prefix.c_str(), a.frames);
     if (!a.save.empty() && fvb_save(s, a.save.c_str())) std::fprintf(stderr, "save: %s\n", fvb_last_error());
     fvb_destroy(s);

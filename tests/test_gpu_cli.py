@@ -92,6 +92,21 @@ def test_fvb_up7_order9(tmp_path, args, order, flux):
     assert np.array_equal(c.get_state(layout="cons", interior=True), s.get_state(layout="cons", interior=True))
 
 
+def test_fvb_up7_metrics_lines(tmp_path):
+    """--metrics: one JSON line per frame and one at the end, with the step,
+    time and throughput of the run"""
+    import json
+    r = subprocess.run([str(BIN / "fvb_up7"), "64", "--t-end", "0.02", "--frames", "2", "--no-ppm", "--metrics",
+                        "m.jsonl"], cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(x) for x in (tmp_path / "m.jsonl").read_text().splitlines()]
+    assert [x["event"] for x in lines] == ["frame", "frame", "done"]
+    assert lines[0]["t"] == pytest.approx(0.01, abs=1e-15) and lines[-1]["t"] == pytest.approx(0.02, abs=1e-15)
+    assert lines[0]["step"] < lines[1]["step"] == lines[2]["step"]
+    assert all(x["n"] == 64 and x["precision"] == "f64" and x["cell_stage_per_s"] > 0 for x in lines)
+    assert lines[-1]["hbm_gbs"] == pytest.approx(lines[-1]["cell_stage_per_s"] * 256 / 3 / 1e9, rel=1e-5)
+
+
 def test_fvb_up7_frames(tmp_path):
     r = subprocess.run([str(BIN / "fvb_up7"), "48", "--t-end", "0.02", "--frames", "2", "--bin"], cwd=tmp_path,
                        capture_output=True, text=True, timeout=120)
