@@ -25,6 +25,8 @@ extern "C" fvb_status fvb_serve_run(const fvb_serve_config *cfg, const fvb_reque
 {
     NvtxRange nvtx_range("fvb_serve_run");
     if (!cfg || (!reqs && nreq) || (!res && nreq) || nreq < 0) return fail(FVB_ERR_INVALID, "bad argument");
+    if ((cfg->policy != FVB_SERVE_FIFO && cfg->policy != FVB_SERVE_SHORTEST_FIRST) || !(cfg->max_cells >= 0.0))
+        return fail(FVB_ERR_INVALID, "unknown admission policy %d or negative cell cap", cfg->policy);
     fvb_batch *b = nullptr;
     fvb_status st = fvb_batch_create(&cfg->batch, &b);
     if (st) return st;

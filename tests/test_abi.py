@@ -79,6 +79,13 @@ def test_invalid_configs_rejected(kw):
     assert e.value.status == L.ERR_INVALID
 
 
+@pytest.mark.parametrize("policy,max_cells", [(7, 0.0), (0, -1.0), (1, float("nan"))])
+def test_serve_config_validated(policy, max_cells):
+    cfg = L.ServeConfig()
+    cfg.policy, cfg.max_cells = policy, max_cells
+    assert F.lib().fvb_serve_run(C.byref(cfg), None, 0, None, None) == L.ERR_INVALID
+
+
 def test_kernel_contract_validates_geometry():
     st = F.lib().fvb_up_rhs(1, 1, 1, 16, 20, 7, 0.1, 1.4, 1, None)  # np < n + 2g
     assert st == L.ERR_INVALID
