@@ -201,8 +201,9 @@ def test_batch_bad_instances_stay_isolated(prec):
 
 # --- serving loop ---------------------------------------------------------------
 
-@pytest.mark.parametrize("policy,max_cells", [("fifo", 0), ("shortest", 12000)])
-def test_serve_stream_matches_alone(policy, max_cells):
+@pytest.mark.parametrize("policy,max_cells,prec", [("fifo", 0, "f32c"), ("shortest", 12000, "f32c"),
+                                                   ("shortest", 12000, "f64")])
+def test_serve_stream_matches_alone(policy, max_cells, prec):
     """Every request of a stream finishes at its t_end with the state the
     same grid reaches alone, bit for bit, whatever joined it on the device;
     with a cell cap the live instances never hold more than the cap (but
@@ -216,13 +217,13 @@ def test_serve_stream_matches_alone(policy, max_cells):
         d, c = _desc(n, 500 + k, float(rng.uniform(0.02, 0.06)))
         reqs.append((t, d))
         cases.append(c)
-    res, wall = F.serve_run(reqs, precision="f32c", steps_per_round=4, policy=policy, max_cells=max_cells,
+    res, wall = F.serve_run(reqs, precision=prec, steps_per_round=4, policy=policy, max_cells=max_cells,
                             keep_results=True)
     assert all(r["status"] == 0 and r["finished"] >= r["admitted"] >= 0 for r in res)
     for (arr, d), r, c in zip(reqs, res, cases):
         assert r["admitted"] >= arr - 1e-3
         assert abs(r["t"] - d.t_end) <= 1e-12
-        s = F.Solver(d.n, precision="f32c", bc="transmissive", cfl=0.5)
+        s = F.Solver(d.n, precision=prec, bc="transmissive", cfl=0.5)
         s.init_case(c)
         s.advance(d.t_end)
         assert s.sync().steps == r["steps"]
@@ -236,8 +237,8 @@ def test_serve_stream_matches_alone(policy, max_cells):
                        if j != i and o["admitted"] <= res[i]["admitted"] < o["finished"])
             assert live == 0 or live + d.n ** 2 <= max_cells, (i, live)
     lat = sorted(r["finished"] - r["arrival"] for r in res)
-    print("serve %s: %d requests in %.3f s, p50 %.4f s p99 %.4f s" % (policy, len(res), wall, lat[len(lat) // 2],
-                                                                        lat[-1]))
+    print("serve %s %s: %d requests in %.3f s, p50 %.4f s p99 %.4f s" % (policy, prec, len(res), wall,
+                                                                           lat[len(lat) // 2], lat[-1]))
 
 
 def test_solvers_on_concurrent_host_threads():
