@@ -240,8 +240,10 @@ def measure_form(F, torch, stream, precision, n, steps, warmup, dist):
 
 def e2e_run(F, torch, stream, precision, n, steps, dist):
     """Through the public API with host buffers: upload the initial state from
-    pinned host memory, then per step one fvb_step and one fvb_sync (the D2H
-    read of the step's t, dt and lam_max), then download the final state."""
+    pinned host memory, then per step one fvb_step and the D2H read of that
+    step's t, dt and lam_max (fvb_stats_post behind the step, fvb_stats_wait
+    for it while the next step runs; the last one is waited for before the
+    download), then download the final state."""
     sys.path.insert(0, str(ROOT / "tests"))
     from cases import kh
     host_in = torch.from_numpy(kh(n)).pin_memory()
@@ -255,9 +257,14 @@ def e2e_run(F, torch, stream, precision, n, steps, dist):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s.set_state(host_in.numpy(), interior=True)
-    for _ in range(steps):
+    for k in range(steps):
         s.step(1)
-        s.sync()
+        s.post_stats(k % 2)
+        if k:
+            st = s.wait_stats((k - 1) % 2)
+            if st.status:
+                raise RuntimeError("step %d stopped with status %d" % (k, st.status))
+    s.wait_stats((steps - 1) % 2)
     s.get_state(interior=True, out=host_out.numpy())
     t1 = time.perf_counter()
     sec = R.max_over_ranks(t1 - t0, dist)
@@ -318,8 +325,9 @@ def run_gpu(args):
         sec, bi, bo = e2e_run(F, torch, stream, args.precision, n, K, dist)
         line["e2e"] = {"value": world * units / sec, "unit": "cell-stage updates/s",
                        "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
-                       "how": "fvb_set_state from pinned host memory, then per step fvb_step + fvb_sync "
-                              "(D2H of t/dt/lam_max), then fvb_get_state to pinned host memory; wall clock"}
+                       "how": "fvb_set_state from pinned host memory, then per step fvb_step + fvb_stats_post "
+                              "(D2H of t/dt/lam_max, waited for while the next step runs), then fvb_get_state "
+                              "to pinned host memory; wall clock"}
 
     if rank == 0 and not args.no_cpu:
         rate, kind, threads, sec = cpu_reference_rate(min(n, 512), 4, 1)

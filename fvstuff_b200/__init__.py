@@ -226,6 +226,16 @@ class Solver:
         check(lib().fvb_sync(self._h, C.byref(s)), "fvb_sync")
         return Stats.from_c(s)
 
+    def post_stats(self, slot: int = 0) -> None:
+        """Enqueue a read of the step control behind the steps enqueued so far."""
+        check(lib().fvb_stats_post(self._h, int(slot)), "fvb_stats_post")
+
+    def wait_stats(self, slot: int = 0) -> Stats:
+        """Wait for the read posted to `slot` (not for later steps)."""
+        s = L.Stats()
+        check(lib().fvb_stats_wait(self._h, int(slot), C.byref(s)), "fvb_stats_wait")
+        return Stats.from_c(s)
+
     def stats(self) -> Stats:
         s = L.Stats()
         check(lib().fvb_stats_sums(self._h, C.byref(s)), "fvb_stats_sums")

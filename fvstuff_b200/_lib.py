@@ -92,6 +92,8 @@ _SIG = {
     "fvb_step": (C.c_int, [_P, C.c_int, C.c_double]),
     "fvb_advance": (C.c_int, [_P, C.c_double, C.c_int64, C.c_int]),
     "fvb_sync": (C.c_int, [_P, C.POINTER(Stats)]),
+    "fvb_stats_post": (C.c_int, [_P, C.c_int]),
+    "fvb_stats_wait": (C.c_int, [_P, C.c_int, C.POINTER(Stats)]),
     "fvb_stats_sums": (C.c_int, [_P, C.POINTER(Stats)]),
     "fvb_set_graph": (C.c_int, [_P, C.c_int]),
     "fvb_up_rhs": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _P]),

@@ -157,6 +157,10 @@ struct fvb_solver {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t frame_ready = nullptr, frame_copied = nullptr;
     bool frame_pending = false, frame_used = false;
+    // posted step-control reads (fvb_stats_post / fvb_stats_wait)
+    Ctrl *stats_ring = nullptr;  // pinned, FVB_STATS_SLOTS entries
+    cudaEvent_t stats_ev[FVB_STATS_SLOTS] = {};
+    bool stats_posted[FVB_STATS_SLOTS] = {};
 };
 
 static fvb_status ensure_staging(fvb_solver *s)
@@ -439,6 +443,9 @@ void fvb_destroy(fvb_solver *s)
     if (s->frame_host) cudaFreeHost(s->frame_host);
     if (s->frame_ready) cudaEventDestroy(s->frame_ready);
     if (s->frame_copied) cudaEventDestroy(s->frame_copied);
+    if (s->stats_ring) cudaFreeHost(s->stats_ring);
+    for (cudaEvent_t ev : s->stats_ev)
+        if (ev) cudaEventDestroy(ev);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -720,23 +727,49 @@ fvb_status fvb_step(fvb_solver *s, int nsteps, double t_stop)
     return FVB_OK;
 }
 
+static void stats_from_ctrl(const Ctrl &c, fvb_stats *st)
+{
+    std::memset(st, 0, sizeof *st);
+    st->t = c.t;
+    st->dt = c.dt;
+    unsigned long long b = c.lam_acc;
+    std::memcpy(&st->lam_max, &b, sizeof b);
+    st->t_stop = c.t_stop;
+    st->steps = c.step;
+    st->status = c.status;
+}
+
 fvb_status fvb_sync(fvb_solver *s, fvb_stats *st)
 {
     if (!s) return fail(FVB_ERR_INVALID, "null solver");
     cudaError_t e = cudaMemcpyAsync(s->ctrl_host, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) return cuda_fail(e, "sync");
-    if (st) {
-        std::memset(st, 0, sizeof *st);
-        const Ctrl &c = *s->ctrl_host;
-        st->t = c.t;
-        st->dt = c.dt;
-        unsigned long long b = c.lam_acc;
-        std::memcpy(&st->lam_max, &b, sizeof b);
-        st->t_stop = c.t_stop;
-        st->steps = c.step;
-        st->status = c.status;
-    }
+    if (st) stats_from_ctrl(*s->ctrl_host, st);
+    return FVB_OK;
+}
+
+fvb_status fvb_stats_post(fvb_solver *s, int slot)
+{
+    if (!s || slot < 0 || slot >= FVB_STATS_SLOTS) return fail(FVB_ERR_INVALID, "null solver or bad slot %d", slot);
+    cudaError_t e = cudaSuccess;
+    if (!s->stats_ring) e = cudaMallocHost(&s->stats_ring, sizeof(Ctrl) * FVB_STATS_SLOTS);
+    if (e == cudaSuccess && !s->stats_ev[slot]) e = cudaEventCreateWithFlags(&s->stats_ev[slot], cudaEventDisableTiming);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->stats_ring + slot, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(s->stats_ev[slot], s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "stats post");
+    s->stats_posted[slot] = true;
+    return FVB_OK;
+}
+
+fvb_status fvb_stats_wait(fvb_solver *s, int slot, fvb_stats *st)
+{
+    if (!s || !st || slot < 0 || slot >= FVB_STATS_SLOTS) return fail(FVB_ERR_INVALID, "bad argument");
+    if (!s->stats_posted[slot]) return fail(FVB_ERR_INVALID, "nothing posted to slot %d", slot);
+    const cudaError_t e = cudaEventSynchronize(s->stats_ev[slot]);
+    if (e != cudaSuccess) return cuda_fail(e, "stats wait");
+    stats_from_ctrl(s->stats_ring[slot], st);
     return FVB_OK;
 }
 

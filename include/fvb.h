@@ -198,6 +198,15 @@ FVB_API fvb_status fvb_step(fvb_solver *s, int nsteps, double t_stop);
 FVB_API fvb_status fvb_advance(fvb_solver *s, double t_stop, int64_t max_steps, int chunk);
 /* Wait for the stream and read the step control (t, dt, lam_max, status). */
 FVB_API fvb_status fvb_sync(fvb_solver *s, fvb_stats *st);
+/* The same read without waiting for later work: fvb_stats_post enqueues a
+ * copy of the step control, as it stands after the steps enqueued so far,
+ * into slot `slot` (0 .. FVB_STATS_SLOTS-1) of a pinned ring;
+ * fvb_stats_wait waits for that copy only and fills st.  A caller can post
+ * after each fvb_step and wait for the previous step's slot while the next
+ * step runs.  A slot is reused by its next post. */
+#define FVB_STATS_SLOTS 8
+FVB_API fvb_status fvb_stats_post(fvb_solver *s, int slot);
+FVB_API fvb_status fvb_stats_wait(fvb_solver *s, int slot, fvb_stats *st);
 
 /* The rec3 family's count of 2x2 blocks whose mean itself needed the floor
  * fix (the "brutal mean-fix activations" fv_rec3_2d.cu:250, :594 reports),

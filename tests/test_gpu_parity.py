@@ -304,6 +304,31 @@ def test_graph_and_direct_launches_agree_bitwise():
     assert np.array_equal(a.get_state(), b.get_state())
 
 
+def test_posted_stats_match_sync():
+    """fvb_stats_post / fvb_stats_wait give each step's control as fvb_sync
+    does, read while later steps are enqueued"""
+    n = 64
+    a = F.Solver(n, bc="periodic", cfl=0.5)
+    b = F.Solver(n, bc="periodic", cfl=0.5)
+    for s in (a, b):
+        s.set_state(riemann4(n, seed=8), interior=True)
+    posted = []
+    for k in range(12):
+        a.step(1)
+        a.post_stats(k % 3)
+        if k >= 2:
+            posted.append(a.wait_stats((k - 2) % 3))
+    posted += [a.wait_stats(10 % 3), a.wait_stats(11 % 3)]
+    for k in range(12):
+        b.step(1)
+        want = b.sync()
+        got = posted[k]
+        assert (got.t, got.dt, got.lam_max, got.steps, got.status) == \
+            (want.t, want.dt, want.lam_max, want.steps, want.status), k
+    with pytest.raises(F.FvbError):
+        F.Solver(n).wait_stats(0)  # nothing posted
+
+
 def test_blowup_reported_not_fatal():
     n = 16
     s = F.Solver(n, bc="periodic")
