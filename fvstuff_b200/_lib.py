@@ -110,6 +110,7 @@ _SIG = {
     "fvb_batch_poll": (C.c_int, [_P, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
     "fvb_batch_get_state": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int, C.c_int]),
     "fvb_batch_instance_stats": (C.c_int, [_P, C.c_int, C.POINTER(Stats)]),
+    "fvb_batch_instance_sums": (C.c_int, [_P, C.c_int, C.POINTER(Stats)]),
     "fvb_batch_remove": (C.c_int, [_P, C.c_int]),
     "fvb_batch_active": (C.c_int, [_P]),
     "fvb_batch_bytes_in_use": (C.c_size_t, [_P]),

@@ -66,10 +66,15 @@ class Batch:
                                         1 if out.dtype == np.float64 else 0, int(interior)), "fvb_batch_get_state")
         return out
 
-    def stats(self, iid: int):
+    def stats(self, iid: int, sums: bool = False):
+        """The instance's step control; with `sums`, also its FP64 conserved
+        sums and non-finite flag."""
         from . import Stats
         s = L.Stats()
-        check(lib().fvb_batch_instance_stats(self._h, iid, C.byref(s)), "fvb_batch_instance_stats")
+        if sums:
+            check(lib().fvb_batch_instance_sums(self._h, iid, C.byref(s)), "fvb_batch_instance_sums")
+        else:
+            check(lib().fvb_batch_instance_stats(self._h, iid, C.byref(s)), "fvb_batch_instance_stats")
         return Stats.from_c(s)
 
     def remove(self, iid: int) -> None:

@@ -48,6 +48,8 @@ struct fvb_batch {
     TileRef *tiles_host = nullptr;  // pinned staging
     int *ntiles_dev = nullptr;
     int *ntiles_host = nullptr;
+    double *sums_dev = nullptr;     // per-block partials of fvb_batch_instance_sums
+    double *sums_host = nullptr;    // pinned
     size_t tiles_cap = 0;
     int shape = 0;
     int ctas = 0;
@@ -244,6 +246,8 @@ void fvb_batch_destroy(fvb_batch *b)
     cudaFree(b->ntiles_dev);
     cudaFreeHost(b->ntiles_host);
     if (b->staging) cudaFree(b->staging);
+    if (b->sums_dev) cudaFree(b->sums_dev);
+    if (b->sums_host) cudaFreeHost(b->sums_host);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -440,6 +444,36 @@ fvb_status fvb_batch_instance_stats(fvb_batch *b, int id, fvb_stats *st)
     st->t_stop = c.t_stop;
     st->steps = c.step;
     st->status = c.status;
+    return FVB_OK;
+}
+
+fvb_status fvb_batch_instance_sums(fvb_batch *b, int id, fvb_stats *st)
+{
+    if (!b || !st) return fail(FVB_ERR_INVALID, "null argument");
+    if (id < 0 || id >= b->max_inst || !b->inst[id].live) return fail(FVB_ERR_NOT_FOUND, "no instance %d", id);
+    constexpr int kBlocks = 592;
+    cudaError_t e = cudaSuccess;
+    if (!b->sums_dev) {
+        e = cudaMalloc(&b->sums_dev, sizeof(double) * 5 * kBlocks);
+        if (e == cudaSuccess) e = cudaMallocHost(&b->sums_host, sizeof(double) * 5 * kBlocks);
+        if (e != cudaSuccess) return cuda_fail(e, "sums buffers");
+    }
+    Instance &I = b->inst[id];
+    const int p = inst_parity(b, I);
+    e = sums_partials(inst_state(b, I, p), I.gd.lo[p], view_of(I.gd), b->internal, I.desc.gamma, b->sums_dev,
+                      kBlocks, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->sums_host, b->sums_dev, sizeof(double) * 5 * kBlocks, cudaMemcpyDeviceToHost,
+                            b->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "sums");
+    const fvb_status r = fvb_batch_instance_stats(b, id, st);  // waits for the stream
+    if (r) return r;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int k = 0; k < kBlocks; ++k)
+        for (int q = 0; q < 5; ++q) acc[q] += b->sums_host[k * 5 + q];
+    const double h2 = I.gd.h * I.gd.h;
+    for (int q = 0; q < 4; ++q) st->sums[q] = acc[q] * h2;
+    st->nonfinite = acc[4] > 0;
     return FVB_OK;
 }
 

@@ -304,6 +304,9 @@ FVB_API fvb_status fvb_batch_run(fvb_batch *b, int nsteps);
 FVB_API fvb_status fvb_batch_poll(fvb_batch *b, int *ids, int cap, int *n_done);
 FVB_API fvb_status fvb_batch_get_state(fvb_batch *b, int id, void *dst, int layout, int dtype, int interior_only);
 FVB_API fvb_status fvb_batch_instance_stats(fvb_batch *b, int id, fvb_stats *st);
+/* as fvb_batch_instance_stats, plus the instance's FP64 conserved sums and
+ * its non-finite flag (what fvb_stats_sums gives for a solver) */
+FVB_API fvb_status fvb_batch_instance_sums(fvb_batch *b, int id, fvb_stats *st);
 FVB_API fvb_status fvb_batch_remove(fvb_batch *b, int id);
 FVB_API int fvb_batch_active(const fvb_batch *b);
 FVB_API size_t fvb_batch_bytes_in_use(const fvb_batch *b);

@@ -117,6 +117,8 @@ def test_batched_512_riemann_instances():
             continue
         assert st.t == pytest.approx(t_end, rel=0, abs=1e-12)
         w = b.get_state(iid, n)
+        # the batch's own non-finite flag tells the caller what the state shows
+        assert b.stats(iid, sums=True).nonfinite == (not np.all(np.isfinite(w))), k
         if not np.all(np.isfinite(w)):
             # the step control stops on a non-finite or non-positive global
             # wave-speed maximum only, and that maximum skips NaN cells (as
@@ -154,9 +156,12 @@ def test_batched_512_riemann_instances():
         sa = s.sync()
         assert (sa.status, sa.steps) == (st.status, st.steps), (k, n)
         # what tells the caller of a finished grid: the non-finite flag of
-        # the conserved sums
+        # the conserved sums, the same for the grid alone and in the batch
         if st.status == 0:
-            assert s.stats().nonfinite == (k in nonfinite), (k, n)
+            alone, mixed = s.stats(), b.stats(ids[k], sums=True)
+            assert alone.nonfinite == mixed.nonfinite == (k in nonfinite), (k, n)
+            if not alone.nonfinite:
+                assert alone.sums == mixed.sums, (k, n)
         assert np.array_equal(b.get_state(ids[k], n), s.get_state(interior=True), equal_nan=True), (k, n)
         s.close()
     for iid in ids:
