@@ -12,8 +12,6 @@
 //
 // The same stage kernel as fvb_step runs here, with plain (non-TMA) loads
 // because the caller's IDX_P rows need not be 16-byte aligned.
-#include <mutex>
-
 #include "fvb_host.h"
 
 namespace fvb {
@@ -28,25 +26,18 @@ constexpr size_t kScratchDoubles = kCtrlDoubles + 2 * 4 * kPlanePad;
 // step control, then the stage-1 and stage-2 outputs (4 planes each)
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-// device address of the array, looked up once per device with that device
-// current (in host code the symbol is only a host-side stand-in)
-std::mutex g_mu;
-double *g_addr[64] = {nullptr};
-
-fvb_status scratch_for_current_device(double **out)
+// Device address of the array in the CUDA context current on this thread.
+// In host code the symbol is only a host-side stand-in, and the address
+// belongs to one context: after cudaDeviceReset, or under a caller's own
+// non-primary context on the same device, a cached address would be stale.
+// So it is looked up on every call (a table lookup in the runtime, small
+// next to the launches that follow).
+fvb_status scratch_for_current_context(double **out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if (dev < 0 || dev >= 64) return fail(FVB_ERR_INVALID, "device ordinal %d out of range", dev);
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
-        g_addr[dev] = (double *)p;
-    }
-    *out = g_addr[dev];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
+    *out = (double *)p;
     return FVB_OK;
 }
 
@@ -67,7 +58,7 @@ extern "C" fvb_status fvb_step_noalloc(double *Qp, int n, int np, double h, doub
     if (nsteps < 0 || bc_x < 0 || bc_x > 2 || bc_y < 0 || bc_y > 2 || !(h > 0) || !(cfl > 0) || !(gamma > 1))
         return fail(FVB_ERR_INVALID, "fvb_step_noalloc: bad step count, boundary condition, h, cfl or gamma");
     double *scratch = nullptr;
-    fvb_status r = scratch_for_current_device(&scratch);
+    fvb_status r = scratch_for_current_context(&scratch);
     if (r) return r;
     cudaStream_t s = (cudaStream_t)stream;
 
