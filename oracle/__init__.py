@@ -415,11 +415,26 @@ def ref_up_ic_sod(N: int, h: float, dtype=np.float64) -> np.ndarray:
     return U
 
 
+def ref_native() -> C.CDLL | None:
+    """The reference's FP64 kernels built for speed on this machine
+    (``-O3 -march=native``, contraction allowed; oracle/build.py
+    ``build_timing``): the timed CPU baseline, never a checker.  None when the
+    extracted reference source is absent or the compiler fails."""
+    from . import build as _b
+    try:
+        p = _b.build_timing()
+    except (RuntimeError, OSError):
+        return None
+    return _load(p) if p is not None else None
+
+
 def ref_up_run(U: np.ndarray, N: int, h: float, cfl: float, bc_kind: int, max_steps: int,
-               t_stop: float = 1e30):
+               t_stop: float = 1e30, lib: C.CDLL | None = None):
+    """The reference's own SSP-RK3 loop on the host (U in place); `lib` picks
+    another build of the same kernels (ref_native)."""
     s = _sfx(U.dtype)
     info = np.zeros(4)
-    st = getattr(ref_host("up7_" + s), "ref_up7_run_" + s)(
+    st = getattr(lib if lib is not None else ref_host("up7_" + s), "ref_up7_run_" + s)(
         _ptr(U), C.c_int(N), _real(U.dtype)(h), _real(U.dtype)(cfl), C.c_int(bc_kind), C.c_int(max_steps),
         C.c_double(t_stop), _ptr(info))
     return int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3])
@@ -519,3 +534,31 @@ def refg_rec3_run(U: np.ndarray, N: int, h: float, cfl: float, max_steps: int, t
     if st > 0:
         raise RuntimeError("reference GPU run failed: cuda error %d" % st)
     return -int(st), float(info[0]), int(info[1]), float(info[2]), float(info[3]), float(ms.value)
+
+
+def refg_up7_frame(Q: np.ndarray, N: int, h: float, fn: str) -> None:
+    """The reference's frame pipeline (its sensor and derived-field kernels,
+    colour ranges and 2x2 composite writer) on the padded primitive state Q
+    (float32 as shipped, or float64 with the retype), written to `fn`."""
+    s = _sfx(Q.dtype)
+    st = getattr(ref_gpu("up7_" + s), "refg_up7_frame_" + s)(_ptr(np.ascontiguousarray(Q)), C.c_int(N),
+                                                             _real(Q.dtype)(h), str(fn).encode())
+    if st != 0:
+        raise RuntimeError("reference frame failed: cuda error %d" % st)
+
+
+def refg_program(kind: str, args: list[str]) -> list[str]:
+    """Command line that runs the reference program itself -- its main(),
+    unchanged, from the GPU build of `kind` ('up7_f32', 'keep', ...) -- with
+    `args`, in a process of its own (it writes its files into the current
+    directory and its report to stdout)."""
+    import sys
+    lib_path = str(REF / ("libref_gpu_%s.so" % kind))
+    code = ("import ctypes, sys\n"
+            "L = ctypes.CDLL(sys.argv[1])\n"
+            "argv = [b'ref'] + [a.encode() for a in sys.argv[2:]]\n"
+            "arr = (ctypes.c_char_p * len(argv))(*argv)\n"
+            "r = L.refg_main(len(argv), arr)\n"
+            "ctypes.CDLL(None).fflush(None)\n"
+            "sys.exit(r)\n")
+    return [sys.executable, "-c", code, lib_path, *args]

@@ -6,7 +6,8 @@ Two things are built here, both outside the product:
   with ``-ffp-contract=off`` so each operation rounds once, as written.
 * ``oracle/_ref/`` -- the reference solvers' own kernels, compiled from the
   files where they lie in the read-only reference checkout
-  (``FVB_REFERENCE_DIR``, default ``/root/reference``):
+  (``FVB_REFERENCE_DIR``; without it, a ``reference`` folder beside the
+  checkout):
 
   - host builds (g++ + OpenMP) of the device functions and grid-stride
     kernels, taken by line range from the reference source and compiled
@@ -20,6 +21,10 @@ Two things are built here, both outside the product:
 
   Everything generated goes to ``oracle/_ref/`` (git-ignored).  When the
   reference checkout is absent the prebuilt files there are used as they are.
+
+* ``oracle/_ref/libref_host_up7_f64_native.so`` (``build_timing``) -- the
+  same FP64 kernels built for speed on the machine that times them: the CPU
+  baseline, not a checker.
 """
 from __future__ import annotations
 
@@ -31,7 +36,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF_DIR = Path(os.environ.get("FVB_REFERENCE_DIR", "/root/reference"))
+REF_DIR = Path(os.environ.get("FVB_REFERENCE_DIR", str(HERE.parent.parent / "reference")))
 
 UP7 = "fv_up7_ducros_2d.cu"
 KEEP = "keep_fv_euler_2d.cu"
@@ -180,6 +185,54 @@ def build_ref(verbose: bool = False, gpu: bool = True) -> list[Path]:
                     print("built", out)
             built.append(out)
     return built
+
+
+def _cpu_signature() -> str:
+    """CPU model and feature flags of this machine, and the compiler version:
+    a -march=native build is only valid where all three match."""
+    model, flags = "", ""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if not model and line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+            if not flags and line.startswith("flags"):
+                flags = " ".join(sorted(line.split(":", 1)[1].split()))
+            if model and flags:
+                break
+    except OSError:
+        pass
+    cc = subprocess.run(["g++", "--version"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                        text=True).stdout.splitlines()
+    return "%s\n%s\n%s\n" % (model, flags, cc[0] if cc else "")
+
+
+TIMING_LIB = "libref_host_up7_f64_native.so"
+
+
+def build_timing(verbose: bool = False) -> Path | None:
+    """The CPU-baseline build of the reference kernels (FP64 retype of
+    fv_up7_ducros_2d.cu): ``g++ -O3 -march=native -fopenmp`` with the
+    compiler's default floating-point contraction, as a user would build it
+    for speed.  The pin build above keeps ``-ffp-contract=off``, which this
+    one must not inherit.  Built on the machine that times it (the extracted
+    source in ``_ref/`` travels; the reference checkout need not), and
+    rebuilt when the CPU or compiler differs from the one it was built on.
+    Returns None when the extracted source is absent."""
+    inc = OUT / "up7_host_f64.inc"
+    if not inc.exists():
+        return None
+    out, sig_file = OUT / TIMING_LIB, OUT / (TIMING_LIB + ".cpu")
+    sig = _cpu_signature()
+    fresh = not _stale(out, [inc, HERE / "ref_host.cpp", HERE / "ref_shim.h", HERE / "build.py"])
+    if fresh and sig_file.exists() and sig_file.read_text() == sig:
+        return out
+    _run(["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-march=native", "-w", "-I", str(HERE),
+          "-DREF_UP7", "-DREF_REAL=double", "-DREF_SFX=f64", '-DREF_INC="_ref/up7_host_f64.inc"',
+          "-o", str(out), str(HERE / "ref_host.cpp")])
+    sig_file.write_text(sig)
+    if verbose:
+        print("built", out)
+    return out
 
 
 def build(verbose: bool = False, gpu: bool = True) -> None:

@@ -63,10 +63,16 @@ static void harness_bc(R *Q, int N, int Np, int bc)
 {
     int g = (Np - N) / 2;
     long long Np2 = (long long)Np * Np;
+    int nt = g_nthreads > 0 ? g_nthreads : omp_get_max_threads();
+    /* rows in parallel; an interior row only has its 2g ghost columns */
+#pragma omp parallel for num_threads(nt) schedule(static)
     for (int jp = 0; jp < Np; ++jp)
         for (int ip = 0; ip < Np; ++ip) {
             bool gx = ip < g || ip >= N + g, gy = jp < g || jp >= N + g;
-            if (!gx && !gy) continue;
+            if (!gx && !gy) {
+                ip = N + g - 1;
+                continue;
+            }
             int ir = ip, jr = jp;
             if (bc == 1) {
                 if (ip < g) ir = ip + N; else if (ip >= N + g) ir = ip - N;

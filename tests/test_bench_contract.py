@@ -26,3 +26,6 @@ def test_reference_arm_line():
     assert d["cpu_baseline"]["single_thread"]["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
     assert "workload" in d["config"]
+    # the arm times the configuration it prints: the full grid, not a sample
+    assert d["config"]["n"] == 256 and "256x256" in d["cpu_baseline"]["sample"]
+    assert d["config"]["parallelism"] == "single"
