@@ -260,10 +260,13 @@ FVB_API fvb_status fvb_max(const void *x, size_t n, void *out_dev, int dtype, vo
  * The stage buffers and step control live in one fixed __device__ array of
  * the library (about 17 MB, held on every GPU that loads libfvb.so), so
  * calls that overlap on the GPU race with each other.  The ghost ring of Qp
- * is refilled.  The first call on a device looks up the array's address;
+ * is refilled.  Every call looks up the array's address in the current
+ * context (the first one on a device may also load the library's kernels);
  * make that first call before any stream capture on that device.  When st
- * is non-null the call waits for the stream and fills it.  No counterpart
- * in the reference. */
+ * is non-null the call waits for the stream and fills it; st->steps counts
+ * the steps of this call only (fvb_stats of a solver counts from its
+ * creation), st->t is the time reached from t0.  No counterpart in the
+ * reference. */
 FVB_API fvb_status fvb_step_noalloc(double *Qp, int n, int np, double h, double cfl, double gamma, int bc_x,
                                     int bc_y, int nsteps, double t0, double t_stop, void *stream, fvb_stats *st);
 
