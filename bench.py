@@ -58,7 +58,10 @@ def parse():
     p.add_argument("--families", default="up_ducros_hll,up_ducros_roe,keep,rec3,up_hllc_d2av",
                    help="families: which ones")
     p.add_argument("--instances", type=int, default=512, help="batched: number of grids")
-    p.add_argument("--plain-sample", type=int, default=32, help="batched: grids timed on the plain FP64 path")
+    p.add_argument("--plain-sample", type=int, default=0,
+                   help="batched: how many of the grids (evenly spaced) the plain FP64 path runs (0: all)")
+    p.add_argument("--riemann-width", type=float, default=0.0,
+                   help="batched: quadrant interfaces smoothed over this many cells (0: sharp)")
     p.add_argument("--requests", type=int, default=48, help="serve: requests in the stream")
     p.add_argument("--rate", type=float, default=200.0, help="serve: mean arrivals per second")
     p.add_argument("--max-n", type=int, default=2048, help="serve: largest grid side")
@@ -68,6 +71,9 @@ def parse():
     p.add_argument("--max-cells", type=float, default=16e6,
                    help="serve: cap on the live instances' interior cells (0: none)")
     p.add_argument("--no-sequential", action="store_true", help="serve: skip the one-at-a-time FP64 comparison")
+    p.add_argument("--rates", default="1,2,4,6,10",
+                   help="serve: offered loads (requests/s) of the latency sweep, '' for none")
+    p.add_argument("--span", type=float, default=10.0, help="serve: seconds of arrivals per sweep stream")
     a = p.parse_args()
     large = a.mode == "large"
     if a.n is None:
@@ -166,15 +172,28 @@ def traffic_from_profiles(precision: str, n: int):
 # CPU: the reference's own kernels compiled for the host (oracle/_ref)
 # ---------------------------------------------------------------------------
 def cpu_reference_rate(sample_n: int, steps: int, warmup: int, threads: int | None = None):
+    """cell-stage updates/s of the reference's own FP64 kernels and host loop
+    (fv_up7_ducros_2d.cu retyped, oracle/_ref) on the KH case at sample_n^2.
+    The build timed is the speed build (-O3 -march=native, contraction
+    allowed, compiled on this machine); without it the bit-exact pin build,
+    and without either the oracle's C restatement ("port")."""
     import oracle as O
     sys.path.insert(0, str(ROOT / "tests"))
     from cases import kh, pad
     threads = threads or os.cpu_count() or 1
-    O.ref_set_threads(threads)
+    lib, build = None, "port"
+    if O.have_ref_host():
+        lib = O.ref_native()
+        build = "g++ -O3 -march=native -fopenmp" if lib is not None else "g++ -O3 -march=x86-64-v3 " \
+                                                                         "-ffp-contract=off -fopenmp"
+        (lib or O.ref_host("up7_f64")).ref_set_threads(threads)
     kind = "reference" if O.have_ref_host() else "port"
     U = pad(kh(sample_n), 4)
     O.bc(U, sample_n, 4, 1)
-    run = O.ref_up_run if kind == "reference" else (lambda U, n, h, c, b, k: O.up_run(U, n, h, c, b, k))
+    if kind == "reference":
+        run = lambda U, n, h, c, b, k: O.ref_up_run(U, n, h, c, b, k, lib=lib)
+    else:
+        run = lambda U, n, h, c, b, k: O.up_run(U, n, h, c, b, k)
     if warmup:
         run(U, sample_n, 1.0 / sample_n, 0.5, 1, warmup)
     t0 = time.perf_counter()
@@ -185,26 +204,32 @@ def cpu_reference_rate(sample_n: int, steps: int, warmup: int, threads: int | No
     sec = (t2 - t1) - (t1 - t0)  # `steps` steps without the prologue
     sec = max(sec, 1e-9)
     rate = 3.0 * sample_n * sample_n * steps / sec
-    return rate, kind, threads, sec
+    return rate, kind, threads, sec, build
 
 
 def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
+    """The reference arm: the reference's own kernels and loop on the host
+    cores, on the GPU line's configuration (the same n, case, CFL and dt
+    rule), with every host thread.  Under torchrun only rank 0 runs."""
+    rank, world, _ = R.env()
     if rank != 0:
         return
-    sample = min(args.n, 512)
+    n = args.n
+    # timed steps bounded so the arm ends within a few minutes at 2048^2
     steps = max(1, min(args.steps, 20))
-    rate, kind, threads, sec = cpu_reference_rate(sample, steps, min(args.warmup, 2))
-    # the same kernels on one host thread, a smaller sample
-    rate1, _, _, sec1 = cpu_reference_rate(256, 4, 1, threads=1)
+    rate, kind, threads, sec, build = cpu_reference_rate(n, steps, min(args.warmup, 2))
+    # the same kernels on one host thread, on a smaller grid
+    rate1, _, _, sec1, _ = cpu_reference_rate(256, 4, 1, threads=1)
+    cfg = dict(workload(n), parallelism="replicas%d" % world if world > 1 else "single")
     line = {"metric": METRIC, "value": rate, "unit": "cell-stage updates/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / steps * 1e3,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": sec / steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload(args.n), "impl": "reference",
+            "data": "synthetic", "config": cfg, "impl": "reference",
             "cpu_baseline": {"value": rate, "unit": "cell-stage updates/s", "cores": threads, "kind": kind,
-                             "sample": "%d steps of the same KH case on a %dx%d grid (FP64 retype of "
-                                       "fv_up7_ducros_2d.cu kernels, OpenMP over all host threads)"
-                                       % (steps, sample, sample),
+                             "build": build,
+                             "sample": "%d SSP-RK3 steps of the KH case on the full %dx%d grid (FP64 retype of "
+                                       "fv_up7_ducros_2d.cu's kernels and loop, OpenMP over all host threads)"
+                                       % (steps, n, n),
                              "single_thread": {"value": rate1, "cores": 1,
                                                "sample": "4 steps on a 256x256 grid"}},
             "e2e": {"value": rate, "unit": "cell-stage updates/s", "h2d_bytes_per_step": 0,
@@ -268,9 +293,61 @@ def e2e_run(F, torch, stream, precision, n, steps, dist):
     s.get_state(interior=True, out=host_out.numpy())
     t1 = time.perf_counter()
     sec = R.max_over_ranks(t1 - t0, dist)
+    # the two state transfers alone (upload with its layout conversion,
+    # download with its conversion), best of three: with the device time of
+    # the steps they bound what any end-to-end run of this length can reach
+    up, down = [], []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        s.set_state(host_in.numpy(), interior=True)
+        s.sync()
+        b = time.perf_counter()
+        s.get_state(interior=True, out=host_out.numpy())
+        c = time.perf_counter()
+        up.append(b - a)
+        down.append(c - b)
     s.close()
     state_bytes = 4 * n * n * 8
-    return sec, state_bytes / steps + 8, state_bytes / steps + 80
+    return sec, state_bytes / steps + 8, state_bytes / steps + 80, min(up), min(down), state_bytes
+
+
+def small_forms(F, torch, plain_value):
+    """The batched, served and precision forms at sizes that take about a
+    minute together: configuration 3 on 128 of its grids, configuration 4 as
+    a 16-request stream, and the configuration-1 vortex over one period in
+    FP32c against FP64."""
+    out = {}
+    with ClockSampler(0) as clk:
+        insts = riemann_instances(128)
+        b = batched_vs_plain(F, insts, 0.25)
+        b["workload"] = "128 of configuration 3's four-quadrant Riemann grids (sharp interfaces, N 64..512, t=0.25)"
+        b["vs_plain_f64_kh2048"] = b["value"] / plain_value
+        out["batched"] = b
+    out["batched"]["clocks"] = clk.summary()
+    with ClockSampler(0) as clk:
+        out["serve"] = serve_form(F, torch, 16, 200.0, 2048)
+    out["serve"]["clocks"] = clk.summary()
+    with ClockSampler(0) as clk:
+        sys.path.insert(0, str(ROOT / "tests"))
+        from cases import vortex
+        m = 256
+        w0 = vortex(m)
+        res = {}
+        for prec in ("f64", "f32c"):
+            s = F.Solver(m, bc="periodic", x0=-5.0, y0=-5.0, length=10.0, cfl=0.5, precision=prec)
+            s.set_state(w0, layout="prim", interior=True)
+            st = s.advance(10.0)
+            res[prec] = (s.get_state(layout="cons", interior=True), st)
+            s.close()
+        l1, linf = _density_errors(res["f32c"][0][0], res["f64"][0][0])
+        out["precision"] = {"workload": "isentropic vortex 256^2 periodic, one period (t=10), FP32c vs FP64",
+                            "l1_rel_density": l1, "linf_rel_density": linf, "bar_l1": 1e-6,
+                            "conserved_l1_rel": {name: _density_errors(res["f32c"][0][q], res["f64"][0][q])[0]
+                                                 for q, name in enumerate(("rho", "rho_u", "rho_v", "E"))},
+                            "steps_f64": res["f64"][1].steps, "steps_f32c": res["f32c"][1].steps}
+    out["precision"]["clocks"] = clk.summary()
+    return out
 
 
 def run_gpu(args):
@@ -312,27 +389,39 @@ def run_gpu(args):
             "clocks": clk.summary()}
 
     if not args.no_forms and args.precision == "f64":
-        with ClockSampler(local):
+        with ClockSampler(local) as clk2:
             s2, ms2 = measure_form(F, torch, stream, "f32c", n, K, W, dist)
         s2.close()
         ms2 = R.max_over_ranks(ms2, dist)
         v2 = world * units / (ms2 / 1e3)
         a2 = BYTES_PER_CELL_STAGE["f32c"] * n * n / (ms2 / (3 * K) / 1e3) / 1e9
         line["forms"] = {"f32c": {"value": v2, "ms_per_step": ms2 / K, "vs_f64": v2 / value,
-                                  "roofline_achieved_gbs": a2, "roofline_frac": a2 / hbm}}
+                                  "roofline_achieved_gbs": a2, "roofline_frac": a2 / hbm,
+                                  "clocks": clk2.summary()}}
+        if world == 1:
+            # the other north-star forms on small instances of their
+            # configurations, so the default line carries them
+            line["forms"].update(small_forms(F, torch, value))
 
     if not args.no_e2e:
-        sec, bi, bo = e2e_run(F, torch, stream, args.precision, n, K, dist)
+        sec, bi, bo, up_s, down_s, sbytes = e2e_run(F, torch, stream, args.precision, n, K, dist)
         line["e2e"] = {"value": world * units / sec, "unit": "cell-stage updates/s",
                        "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+                       "state_upload_ms": up_s * 1e3, "state_download_ms": down_s * 1e3,
+                       "link_gbs": {"h2d": sbytes / up_s / 1e9, "d2h": sbytes / down_s / 1e9},
+                       # the steps' device time plus the two transfers, unoverlapped:
+                       # the state must be whole on the device before the first dt
+                       # (a max over every cell) and whole after the last stage
+                       "bound_value": world * units / (ms / 1e3 + up_s + down_s),
                        "how": "fvb_set_state from pinned host memory, then per step fvb_step + fvb_stats_post "
                               "(D2H of t/dt/lam_max, waited for while the next step runs), then fvb_get_state "
                               "to pinned host memory; wall clock"}
 
     if rank == 0 and not args.no_cpu:
-        rate, kind, threads, sec = cpu_reference_rate(min(n, 512), 4, 1)
+        rate, kind, threads, sec, build = cpu_reference_rate(n, 2, 0)
         line["cpu_baseline"] = {"value": rate, "unit": "cell-stage updates/s", "cores": threads, "kind": kind,
-                                "sample": "4 SSP-RK3 steps of the KH case on a %dx%d grid" % ((min(n, 512),) * 2)}
+                                "build": build,
+                                "sample": "2 SSP-RK3 steps of the KH case on the full %dx%d grid" % (n, n)}
     R.finish(dist)
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -341,16 +430,18 @@ def run_gpu(args):
 # ---------------------------------------------------------------------------
 # the other configurations: batched (3), serving (4), large grid (5)
 # ---------------------------------------------------------------------------
-def riemann_instances(count, seed=2024):
+def riemann_instances(count, seed=2024, width=0.0):
     """`count` four-quadrant Riemann problems, N uniform in {64, 96, ..., 512},
-    quadrant states from per-instance seeds, transmissive, t_end 0.25."""
+    quadrant states from per-instance seeds, transmissive, t_end 0.25.  The
+    quadrant interfaces are sharp (width 0, as the configuration states);
+    width > 0 smooths them over that many cells."""
     import fvstuff_b200 as F
     rng = np.random.default_rng(seed)
     sizes = list(range(64, 513, 32))
     out = []
     for k in range(count):
         n = int(rng.choice(sizes))
-        c = F.case_params("riemann4", 0.0, 0.0, 1.0, seed=int(rng.integers(1, 2 ** 62)))
+        c = F.case_params("riemann4", 0.0, 0.0, 1.0, seed=int(rng.integers(1, 2 ** 62)), param2=width)
         out.append((n, c))
     return out
 
@@ -368,11 +459,11 @@ def advance_counted(s, t_end):
     return s.sync()
 
 
-def run_plain_f64_alone(F, insts, t_end):
-    """The plain FP64 path, one grid at a time; returns (cell-stages, seconds,
-    grids stopped by the guard)."""
+def plain_f64_each(F, insts, t_end):
+    """The plain FP64 path, one grid at a time: per grid (cell-stages,
+    seconds, status).  Set-up (allocation, initial state) is not timed."""
     import torch
-    work, sec, bad = 0.0, 0.0, 0
+    out = []
     for n, c in insts:
         s = F.Solver(n, bc="transmissive", cfl=0.5, precision="f64")
         s.init_case(c)
@@ -380,11 +471,59 @@ def run_plain_f64_alone(F, insts, t_end):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         st = advance_counted(s, t_end)
-        sec += time.perf_counter() - t0
-        work += 3.0 * n * n * st.steps
-        bad += st.status != 0
+        out.append((3.0 * n * n * st.steps, time.perf_counter() - t0, st.status))
         s.close()
-    return work, sec, bad
+    return out
+
+
+def batch_f32c(F, insts, t_end):
+    """All grids in one FP32c batch (one persistent launch per RK stage,
+    graph-replayed), timed from the first step to the last completion;
+    returns (seconds, per grid (cell-stages, status))."""
+    import torch
+    b = F.Batch(precision="f32c")
+    ids = [b.add(F.Batch.desc(n, c, t_end, bc="transmissive", cfl=0.5)) for n, c in insts]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    done = set()
+    while len(done) < len(ids):
+        b.run(16)
+        done.update(b.poll())
+    sec = time.perf_counter() - t0
+    per = []
+    for iid, (n, _) in zip(ids, insts):
+        st = b.stats(iid)
+        per.append((3.0 * n * n * st.steps, st.status))
+    b.close()
+    return sec, per
+
+
+def batched_vs_plain(F, insts, t_end, plain_sample=None):
+    """Configuration 3 on one GPU: the FP32c batch and the plain FP64 path
+    (each grid alone) on the same grids.  Failures (grids stopped by the
+    reference scheme's blow-up / dt-underflow guard) are counted per form,
+    and the speed-up is taken on the grids both forms finish: the batch is
+    run again on exactly those, against the sum of their FP64 times."""
+    sec, per = batch_f32c(F, insts, t_end)
+    idx = list(range(len(insts)))
+    if plain_sample:
+        idx = idx[:: max(1, len(insts) // plain_sample)]
+    plain = plain_f64_each(F, [insts[i] for i in idx], t_end)
+    both = [i for i, (w, st, k) in zip(idx, plain) if k == 0 and per[i][1] == 0]
+    sec_c, per_c = batch_f32c(F, [insts[i] for i in both], t_end) if both else (0.0, [])
+    keep = set(both)
+    plain_c = [p for i, p in zip(idx, plain) if i in keep]
+    rate_b = sum(w for w, _ in per_c) / sec_c if both else None
+    rate_p = sum(w for w, _, _ in plain_c) / sum(t for _, t, _ in plain_c) if both else None
+    return {"value": sum(w for w, _ in per) / sec, "seconds": sec, "instances": len(insts),
+            "failed_f32c": sum(st != 0 for _, st in per),
+            "plain_f64_compared": len(idx), "failed_f64": sum(k != 0 for _, _, k in plain),
+            "failed_f32c_of_compared": sum(per[i][1] != 0 for i in idx),
+            "common_finishers": len(both),
+            "batched_f32c_common": rate_b, "plain_f64_one_at_a_time_common": rate_p,
+            "ratio_common": rate_b / rate_p if both else None,
+            "failed_means": "stopped by the blow-up / dt-underflow guard of the reference scheme "
+                            "(fv_up7_ducros_2d.cu:997-1007) before t_end"}
 
 
 def run_batched(args):
@@ -395,68 +534,44 @@ def run_batched(args):
     torch.cuda.set_device(local)
     dist = R.init("nccl")
     count = args.instances
-    insts = riemann_instances(count)
+    insts = riemann_instances(count, width=args.riemann_width)
     # N ranks split the instances by work (~N^3: cells x steps)
     mine = [insts[i] for i in R.shard_by_work([float(n) ** 3 for n, _ in insts], rank, world)]
     t_end = 0.25
-    b = F.Batch(precision="f32c")
-    ids = {}
-    # instance set-up (allocation, initial state, descriptors) is not timed,
-    # as the plain path's solver creation and initial state are not
-    for n, c in mine:
-        ids[b.add(F.Batch.desc(n, c, t_end, bc="transmissive", cfl=0.5))] = n
-    torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    t0 = time.perf_counter()
-    done = set()
-    while len(done) < len(ids):
-        b.run(16)
-        done.update(b.poll())
-    sec = time.perf_counter() - t0
-    work, bad = 0.0, 0
-    for iid, n in ids.items():
-        st = b.stats(iid)
-        bad += st.status != 0
-        work += 3.0 * n * n * st.steps
-    b.close()
+    sec, per = batch_f32c(F, mine, t_end)
+    work, bad = sum(w for w, _ in per), sum(st != 0 for _, st in per)
     sec = R.max_over_ranks(sec, dist)
     work = R.sum_over_ranks(work, dist)
     bad = int(R.sum_over_ranks(bad, dist))
-    value = work / sec
-    # the plain FP64 form on the same grids one at a time (per GPU): a seeded
-    # sample of them, the rate scaled to the sample's own work
-    sample = insts[:: max(1, count // args.plain_sample)]
-    my_sample = [sample[i] for i in R.shard_by_work([float(n) ** 3 for n, _ in sample], rank, world)]
-    pw, ps, pbad = run_plain_f64_alone(F, my_sample, t_end)
-    pw = R.sum_over_ranks(pw, dist)
-    ps = R.max_over_ranks(ps, dist)
-    pbad = int(R.sum_over_ranks(pbad, dist))
+    # every form on the same grids (rank 0's share), failures per form
+    cmp = batched_vs_plain(F, mine, t_end, plain_sample=args.plain_sample) if rank == 0 else None
     R.finish(dist)
     if rank != 0:
         return
+    value = work / sec
     line = {"metric": METRIC, "value": value, "unit": "cell-stage updates/s", "n_gpus": world, "steps": None,
             "warmup": 0, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32c",
             "data": "synthetic", "mode": "batched",
-            "config": {"workload": "%d four-quadrant Riemann problems, N in {64..512} step 32, transmissive, "
-                                   "t=0.25, CFL 0.5, one persistent launch per RK stage (graph-replayed); "
-                                   "timed from the first step to the last instance's completion, set-up "
-                                   "excluded as for the plain path" % count,
+            "config": {"workload": "%d four-quadrant Riemann problems (%s interfaces), N in {64..512} step 32, "
+                                   "transmissive, t=0.25, CFL 0.5, one persistent launch per RK stage "
+                                   "(graph-replayed); timed from the first step to the last instance's "
+                                   "completion, set-up excluded as for the plain path"
+                                   % (count, "sharp" if args.riemann_width == 0 else
+                                      "%g-cell tanh" % args.riemann_width),
                        "instances": count, "parallelism": "instances split by work over %d GPU(s)" % world,
-                       "failed": bad, "failed_means": "stopped by the blow-up / dt-underflow guard of the "
-                                                     "reference scheme before t_end; their steps count"},
-            "seconds": sec, "cell_stages": work,
-            "plain_f64_one_at_a_time": {"value": pw / ps, "instances_sampled": len(sample), "seconds": ps,
-                                        "failed": pbad},
-            "batched_f32c_vs_plain_f64": value / (pw / ps)}
+                       "failed": bad},
+            "seconds": sec, "cell_stages": work, "forms_same_grids": cmp}
     print(json.dumps(line), flush=True)
 
 
-def serve_requests(F, count, rate, max_n):
+def serve_requests(F, count, rate, max_n, seed=7):
     """The seeded request stream: Poisson arrivals, half isentropic vortices
-    (periodic [-5,5]^2), half four-quadrant Riemann problems (transmissive
-    [0,1]^2), N log-uniform in [128, max_n], t_end uniform in [0.1, 1]."""
-    rng = np.random.default_rng(7)
+    (periodic [-5,5]^2), half four-quadrant Riemann problems with sharp
+    quadrant interfaces (transmissive [0,1]^2), N log-uniform in [128,
+    max_n], t_end uniform in [0.1, 1]."""
+    rng = np.random.default_rng(seed)
     reqs, t = [], 0.0
     for k in range(count):
         t += rng.exponential(1.0 / rate)
@@ -466,13 +581,56 @@ def serve_requests(F, count, rate, max_n):
             c = F.case_params("vortex", -5.0, -5.0, 10.0)
             d = F.Batch.desc(n, c, t_end, bc="periodic", x0=-5.0, y0=-5.0, length=10.0, cfl=0.5)
         else:
-            c = F.case_params("riemann4", 0.0, 0.0, 1.0, seed=int(rng.integers(1, 2 ** 62)))
+            c = F.case_params("riemann4", 0.0, 0.0, 1.0, seed=int(rng.integers(1, 2 ** 62)), param2=0.0)
             d = F.Batch.desc(n, c, t_end, bc="transmissive", cfl=0.5)
         reqs.append((t, d))
     return reqs
 
 
+def _pct(v, q):
+    v = sorted(v)
+    return v[min(len(v) - 1, int(q * len(v)))] if v else None
+
+
+def serve_form(F, torch, count, rate, max_n, policy="shortest", max_cells=16e6, steps_per_round=16,
+               sequential=True, seed=7):
+    """One served stream on this GPU: `count` requests arriving at `rate`
+    per second, admitted against a 150 GB budget and a cap on live cells;
+    p50 / p99 time to solution, throughput, and the same requests one after
+    another on the plain FP64 path (arrival times respected)."""
+    reqs = serve_requests(F, count, rate, max_n, seed=seed)
+    torch.cuda.synchronize()
+    res, wall = F.serve_run(reqs, precision="f32c", hbm_budget=150 << 30, steps_per_round=steps_per_round,
+                            policy=policy, max_cells=max_cells)
+    lat = [r["finished"] - r["arrival"] for r in res]
+    work = sum(3.0 * d.n * d.n * r["steps"] for (_, d), r in zip(reqs, res))
+    out = {"workload": "Poisson stream, %d requests at %g/s, vortex or seeded Riemann, N log-uniform in [128, %d], "
+                       "t_end U[0.1, 1], 150 GB HBM budget" % (count, rate, max_n),
+           "admission": policy, "max_cells": max_cells, "value": work / wall, "p50_s": _pct(lat, 0.5),
+           "p99_s": _pct(lat, 0.99), "wall_s": wall, "arrival_span_s": reqs[-1][0] if reqs else 0.0,
+           "failed": sum(r["status"] != 0 for r in res)}
+    if sequential:
+        t0 = time.perf_counter()
+        seq_lat, clock = [], 0.0
+        for (arr, d), r in zip(reqs, res):
+            s = F.Solver(d.n, bc={0: "reflect", 1: "periodic", 2: "transmissive"}[d.bc_x], x0=d.x0, y0=d.y0,
+                         length=d.length, cfl=d.cfl, precision="f64")
+            s.init_case(d.ic)
+            a = time.perf_counter()
+            advance_counted(s, d.t_end)
+            clock = max(clock, arr) + (time.perf_counter() - a)
+            seq_lat.append(clock - arr)
+            s.close()
+        seq_wall = time.perf_counter() - t0
+        out["sequential_plain_f64"] = {"value": work / seq_wall, "p50_s": _pct(seq_lat, 0.5),
+                                       "p99_s": _pct(seq_lat, 0.99), "wall_s": seq_wall}
+    return out
+
+
 def run_serve(args):
+    """Configuration 4.  One stream at --rate (with the sequential FP64
+    comparison), then, unless --rates is empty, latency against offered
+    load: a stream per rate, each sized so its arrivals span --span seconds."""
     import torch
 
     import fvstuff_b200 as F
@@ -509,10 +667,19 @@ def run_serve(args):
     seq_wall = R.max_over_ranks(seq_wall, dist)
     work = R.sum_over_ranks(work, dist)
     failed = int(R.sum_over_ranks(failed, dist))
+    # latency against offered load (each rank its own stream, rank 0 reports)
+    sweep = []
+    for lam in [float(x) for x in args.rates.split(",") if x.strip()]:
+        count = max(4, int(round(lam * args.span)))
+        sweep.append(dict(rate=lam, requests=count,
+                          **serve_form(F, torch, count, lam, args.max_n, args.policy, args.max_cells,
+                                       args.steps_per_round, sequential=False, seed=11 + rank)))
+        print("rate %g/s: %d requests over %.1f s, p50 %.3f s, p99 %.3f s, %.2f G/s"
+              % (lam, count, sweep[-1]["arrival_span_s"], sweep[-1]["p50_s"], sweep[-1]["p99_s"],
+                 sweep[-1]["value"] / 1e9), file=sys.stderr, flush=True)
     R.finish(dist)
     if rank != 0:
         return
-    pct = lambda v, q: v[min(len(v) - 1, int(q * len(v)))]
     line = {"metric": METRIC, "value": work / wall, "unit": "cell-stage updates/s", "n_gpus": world,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32c", "data": "synthetic",
             "mode": "serve",
@@ -521,11 +688,11 @@ def run_serve(args):
                                                                                         args.max_n),
                        "admission": args.policy, "max_cells": args.max_cells,
                        "parallelism": "request k served by GPU k mod %d" % world},
-            "p50_s": pct(lat, 0.5), "p99_s": pct(lat, 0.99), "wall_s": wall,
-            "failed": failed}
+            "p50_s": _pct(lat, 0.5), "p99_s": _pct(lat, 0.99), "wall_s": wall,
+            "failed": failed, "latency_vs_offered_load": sweep}
     if seq_lat:
-        line["sequential_plain_f64"] = {"value": work / seq_wall, "p50_s": pct(seq_lat, 0.5),
-                                        "p99_s": pct(seq_lat, 0.99), "wall_s": seq_wall}
+        line["sequential_plain_f64"] = {"value": work / seq_wall, "p50_s": _pct(seq_lat, 0.5),
+                                        "p99_s": _pct(seq_lat, 0.99), "wall_s": seq_wall}
     print(json.dumps(line), flush=True)
 
 
@@ -678,7 +845,7 @@ def run_precision(args):
     # a sample of the batched bench's grids: FP32c in one batch against each
     # grid alone on the plain FP64 path, at t_end (instances stopped early by
     # the reference scheme's guard in either form are listed, not compared)
-    inst = riemann_instances(args.instances)[:: max(1, args.instances // args.plain_sample)]
+    inst = riemann_instances(args.instances, width=args.riemann_width)[:: max(1, args.instances // 32)]
     bt = F.Batch(precision="f32c")
     ids = [bt.add(F.Batch.desc(nn, c, 0.25, bc="transmissive", cfl=0.5)) for nn, c in inst]
     done = set()

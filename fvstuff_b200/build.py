@@ -78,7 +78,11 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     if todo or not LIB.exists() or LIB.stat().st_mtime < _newest(objs):
         # public C-ABI symbols are marked visible in the sources; everything
         # else stays hidden
-        _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs)])
+        # linked under a temporary name and renamed, so a reader never sees
+        # a partly written library
+        tmp = LIB.with_name(LIB.name + ".tmp")
+        _run([NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs)])
+        os.replace(tmp, LIB)
         if verbose:
             print("linked", LIB)
     _build_cli(verbose)
@@ -95,8 +99,10 @@ def _build_cli(verbose: bool) -> None:
         deps = [src, LIB, *cli.glob("*.h")]
         if exe.exists() and exe.stat().st_mtime >= _newest(deps):
             continue
+        tmp = exe.with_name(exe.name + ".tmp")
         _run(["g++", "-O2", "-std=c++17", "-I", str(ROOT / "include"), "-I", str(cli), str(src),
-              "-o", str(exe), "-L", str(PKG), "-lfvb", "-Wl,-rpath,$ORIGIN/.."])
+              "-o", str(tmp), "-L", str(PKG), "-lfvb", "-Wl,-rpath,$ORIGIN/.."])
+        os.replace(tmp, exe)
         if verbose:
             print("built", exe)
 
