@@ -41,7 +41,6 @@ struct fvb_batch {
     std::vector<Instance> inst;
     Ctrl *ctrl_dev = nullptr;       // [max_inst]
     Ctrl *ctrl_host = nullptr;      // pinned mirror
-    TileCtl *ctls_dev = nullptr;    // [max_inst] step control of the stage being launched
     GridDev *desc_dev = nullptr;    // [max_inst]
     GridDev *desc_host = nullptr;   // pinned staging
     TileRef *tiles_dev = nullptr;
@@ -72,7 +71,7 @@ static StageArgs batch_args(const fvb_batch *b, int stage, int parity)
 {
     StageArgs a{};
     a.grids = b->desc_dev;
-    a.ctls = b->ctls_dev;
+    a.ctrls = b->ctrl_dev;
     a.tiles = b->tiles_dev;
     a.ntiles = b->ntiles_dev;
     a.stage = stage;
@@ -84,10 +83,8 @@ static cudaError_t launch_steps(fvb_batch *b, int nsteps)
 {
     for (int k = 0; k < nsteps; ++k) {
         for (int stage = 1; stage <= 3; ++stage) {
-            // every slot's step control for this stage, then the stage
-            cudaError_t e = launch_stage_control(b->prec, b->ctrl_dev, b->max_inst, stage, b->ctls_dev, b->stream);
-            if (e != cudaSuccess) return e;
-            e = launch_stage(b->prec, b->order, b->shape, batch_args(b, stage, b->parity), b->ctas,
+            // (each grid's step control is evaluated inside the stage kernel)
+            cudaError_t e = launch_stage(b->prec, b->order, b->shape, batch_args(b, stage, b->parity), b->ctas,
                                          b->stream);
             if (e != cudaSuccess) return e;
         }
@@ -211,7 +208,6 @@ fvb_status fvb_batch_create(const fvb_batch_config *cfg, fvb_batch **out)
     e = cudaMalloc(&b->ctrl_dev, sizeof(Ctrl) * b->max_inst);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->ctrl_dev, 0, sizeof(Ctrl) * b->max_inst, b->stream);
     if (e == cudaSuccess) e = cudaMallocHost(&b->ctrl_host, sizeof(Ctrl) * b->max_inst);
-    if (e == cudaSuccess) e = cudaMalloc(&b->ctls_dev, sizeof(TileCtl) * b->max_inst);
     if (e == cudaSuccess) e = cudaMalloc(&b->desc_dev, sizeof(GridDev) * b->max_inst);
     if (e == cudaSuccess) e = cudaMallocHost(&b->desc_host, sizeof(GridDev) * b->max_inst);
     if (e == cudaSuccess) e = cudaMalloc(&b->ntiles_dev, sizeof(int));
@@ -238,7 +234,6 @@ void fvb_batch_destroy(fvb_batch *b)
         if (I.block) cudaFree(I.block);
     cudaFree(b->ctrl_dev);
     cudaFreeHost(b->ctrl_host);
-    cudaFree(b->ctls_dev);
     cudaFree(b->desc_dev);
     cudaFreeHost(b->desc_host);
     cudaFree(b->tiles_dev);

@@ -124,54 +124,58 @@ __device__ __forceinline__ bool gd_has_tma(const StageArgs &a)
     return a.grids != nullptr || a.grid.tmap != nullptr;
 }
 
-// Step control of one grid for one stage.  `leader` (one thread of the
-// launch per grid: thread 0 of CTA 0 of a single-grid launch, the
-// stage-control kernel's thread for a batch, thread 0 of the tile-0 CTA of
-// the KEEP and rec3 kernels) also writes the stage's control updates: dt,
-// `active` and `clamped` in stage 1, the wave-speed accumulator reset in
-// stage 2.  Every other caller only reads.
+// Step control of one grid for one stage, evaluated from `s`, a copy of the
+// grid's Ctrl taken during this stage (or the Ctrl itself), with the
+// control writes going to `c`.  `leader` (one thread of the launch per grid:
+// thread 0 of CTA 0 of a single-grid launch, the thread that publishes the
+// header of the grid's tile 0 in a batched launch, thread 0 of the tile-0
+// CTA of the KEEP and rec3 kernels) also writes the stage's control updates:
+// dt, `active` and `clamped` in stage 1, the wave-speed accumulator reset in
+// stage 2.  Every other caller only reads.  The fields a stage reads are
+// never written during it, except `status` in stage 1, which the leader may
+// set to a stop that every reader derives for itself from the same inputs.
 template <int PREC>
-__device__ TileCtl tile_control(Ctrl *c, int stage, bool leader)
+__device__ TileCtl step_control(const Ctrl &s, Ctrl *c, int stage, bool leader)
 {
-    TileCtl s{0.0, 0, 0};
-    if (stage == 0) { s.run = 1; return s; }
+    TileCtl k{0.0, 0, 0};
+    if (stage == 0) { k.run = 1; return k; }
     if (stage == 1) {
-        double t = c->t, ts = c->t_stop;
-        if (c->status != 0 || !(t < ts)) {
+        double t = s.t, ts = s.t_stop;
+        if (s.status != 0 || !(t < ts)) {
             if (leader) c->active = 0;
-            return s;
+            return k;
         }
-        double lam = __longlong_as_double((long long)c->lam_acc);
+        double lam = __longlong_as_double((long long)s.lam_acc);
         if (!(lam > 0.0)) {
             if (leader) { c->status = FVB_ERR_BLOWUP; c->active = 0; }
-            return s;
+            return k;
         }
         double dt;
         int clamped = 0;
         if (PREC == P64) {
-            dt = c->cfl * c->h / lam;
+            dt = s.cfl * s.h / lam;
             if (t + dt > ts) { dt = ts - t; clamped = 1; }
             if (dt < 1e-14) {
                 if (leader) { c->status = FVB_ERR_DT_UNDERFLOW; c->active = 0; }
-                return s;
+                return k;
             }
         } else if (PREC == P32) {
             // float time and dt, as the shipped solver keeps them
             float tf = (float)t, tsf = (float)ts;
-            float d = (float)c->cfl * (float)c->h / (float)lam;
+            float d = (float)s.cfl * (float)s.h / (float)lam;
             if (tf + d > tsf) { d = tsf - tf; clamped = 1; }
             if (d < 1e-14f) {
                 if (leader) { c->status = FVB_ERR_DT_UNDERFLOW; c->active = 0; }
-                return s;
+                return k;
             }
             dt = d;
         } else {
             // FP32 dt, FP64 accumulated time landing exactly on t_stop
-            float d = (float)(c->cfl * c->h) / (float)lam;
+            float d = (float)(s.cfl * s.h) / (float)lam;
             if (t + (double)d > ts) { d = (float)(ts - t); clamped = 1; }
             if (d < 1e-14f) {
                 if (leader) { c->status = FVB_ERR_DT_UNDERFLOW; c->active = 0; }
-                return s;
+                return k;
             }
             dt = d;
         }
@@ -179,31 +183,44 @@ __device__ TileCtl tile_control(Ctrl *c, int stage, bool leader)
             c->dt = dt;
             c->active = 1;
             c->clamped = clamped;
-            c->lam_cur = c->lam_acc;
+            c->lam_cur = s.lam_acc;
         }
-        s.dt = dt;
-        s.run = 1;
-        return s;
+        k.dt = dt;
+        k.run = 1;
+        return k;
     }
-    if (!c->active) {
-        s.copy = (stage == 3 && PREC == P32C);
-        return s;
+    if (!s.active) {
+        k.copy = (stage == 3 && PREC == P32C);
+        return k;
     }
-    s.dt = c->dt;
-    s.run = 1;
+    k.dt = s.dt;
+    k.run = 1;
     if (stage == 2 && leader) c->lam_acc = 0ull;
-    return s;
+    return k;
+}
+
+template <int PREC>
+__device__ __forceinline__ TileCtl tile_control(Ctrl *c, int stage, bool leader)
+{
+    return step_control<PREC>(*c, c, stage, leader);
+}
+
+// end of stage 3 (leader): time and step count advance
+template <int PREC>
+__device__ __forceinline__ void leader_finish_from(const Ctrl &s, Ctrl *c)
+{
+    double t = s.t, dt = s.dt;
+    if (PREC == P32) t = (double)((float)t + (float)dt);
+    else if (PREC == P32C) t = s.clamped ? s.t_stop : t + dt;
+    else t = t + dt;
+    c->t = t;
+    c->step = s.step + 1;
 }
 
 template <int PREC>
 __device__ __forceinline__ void leader_finish(Ctrl *c)
 {
-    double t = c->t, dt = c->dt;
-    if (PREC == P32) t = (double)((float)t + (float)dt);
-    else if (PREC == P32C) t = c->clamped ? c->t_stop : t + dt;
-    else t = t + dt;
-    c->t = t;
-    c->step = c->step + 1;
+    leader_finish_from<PREC>(*c, c);
 }
 
 }  // namespace fvb

@@ -77,7 +77,7 @@ struct TileCtl {
 struct StageArgs {
     GridDev grid;              // single-grid launches
     const GridDev *grids;      // batched launches: grid descriptors
-    const TileCtl *ctls;       // batched launches: step control of each grid
+    Ctrl *ctrls;               // batched launches: step control of each grid (indexed like grids)
     const TileRef *tiles;      // batched launches: tile table
     const int *ntiles;         // batched launches: live tile count (device)
     int ntiles_static;         // single-grid launches: tiles
@@ -107,11 +107,10 @@ cudaError_t put_tile_maps(const CUtensorMap maps[TM_COUNT], CUtensorMap *dst, cu
 void *stage32c_fn(int shape, bool batched);
 size_t stage32c_smem(int shape);
 
-// Step control of `count` grids for one stage of a batched launch
-// (fvb_stage.cu): evaluates each grid's Ctrl, applies the stage's control
-// writes (dt in stage 1, the wave-speed accumulator reset in stage 2, the
-// time / step advance in stage 3) and writes the TileCtl the stage reads.
-cudaError_t launch_stage_control(int prec, Ctrl *ctrl, int count, int stage, TileCtl *out, cudaStream_t s);
+// the FP64 stage kernel laid out for three CTAs per SM (fvb_stage64.cu):
+// null where it is not instantiated (order, solver)
+void *stage64_fn(int order, int shape, int rs, bool batched);
+size_t stage64_smem(int order, int shape);
 
 // launchers (fvb_stage.cu).  rs: the solver on the reconstructed states of
 // the FP64 UP7 kernel -- 0 HLLC, 1 HLL, 2 Roe

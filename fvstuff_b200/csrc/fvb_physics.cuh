@@ -111,15 +111,25 @@ __device__ __forceinline__ void upface(const R *s, R &vL, R &vR)
     }
 }
 
-// HLLC with Davis wave-speed bounds, normal frame
+// total energy of a normal-frame state with the kinetic term summed in the
+// Cartesian order u^2 + v^2, as the reference sums it for every face: for a
+// y-face (YF) the normal component is v, so the tangential square comes
+// first (the two orders round differently under a fused multiply-add)
+template <bool YF, class R>
+__device__ __forceinline__ R etot_cart(R r, R un, R ut, R p, const Gas<R> &gs)
+{
+    return YF ? etot(r, ut, un, p, gs) : etot(r, un, ut, p, gs);
+}
+
+// HLLC with Davis wave-speed bounds, normal frame (YF: a y-face)
 //                                               fv_up7_ducros_2d.cu:237-292
-template <class R>
+template <class R, bool YF = false>
 __device__ __forceinline__ void hllc(const R L[4], const R Rr[4], R F[4], const Gas<R> &gs)
 {
     R rL = L[0], uL = L[1], tL = L[2], pL = L[3];
     R rR = Rr[0], uR = Rr[1], tR = Rr[2], pR = Rr[3];
     R cL = sound(pL, rL, gs), cR = sound(pR, rR, gs);
-    R EL = etot(rL, uL, tL, pL, gs), ER = etot(rR, uR, tR, pR, gs);
+    R EL = etot_cart<YF>(rL, uL, tL, pL, gs), ER = etot_cart<YF>(rR, uR, tR, pR, gs);
     R SL = dmin<R>(uL - cL, uR - cR);
     R SR = dmax<R>(uL + cL, uR + cR);
     const R zero = R(0);
@@ -145,15 +155,15 @@ __device__ __forceinline__ void hllc(const R L[4], const R Rr[4], R F[4], const 
     F[3] = (EK + pK) * uK + SK * (Us3 - EK);
 }
 
-// HLLE on the two adjacent cell averages, normal frame
+// HLLE on the two adjacent cell averages, normal frame (YF: a y-face)
 //                                               fv_up7_ducros_2d.cu:296-328
-template <class R>
+template <class R, bool YF = false>
 __device__ __forceinline__ void hlle(const R L[4], const R Rr[4], R F[4], const Gas<R> &gs)
 {
     R rL = L[0], uL = L[1], tL = L[2], pL = L[3];
     R rR = Rr[0], uR = Rr[1], tR = Rr[2], pR = Rr[3];
     R cL = sound(pL, rL, gs), cR = sound(pR, rR, gs);
-    R EL = etot(rL, uL, tL, pL, gs), ER = etot(rR, uR, tR, pR, gs);
+    R EL = etot_cart<YF>(rL, uL, tL, pL, gs), ER = etot_cart<YF>(rR, uR, tR, pR, gs);
     R FL0 = rL * uL, FL1 = rL * uL * uL + pL, FL2 = rL * uL * tL, FL3 = (EL + pL) * uL;
     R FR0 = rR * uR, FR1 = rR * uR * uR + pR, FR2 = rR * uR * tR, FR3 = (ER + pR) * uR;
     R SL = dmin<R>(uL - cL, uR - cR);
@@ -373,19 +383,16 @@ __device__ __forceinline__ void roe_fast(const R L[4], const R Rv[4], const GasF
     Fh[3] = R(0.5) * ((EL + pL) * uL + (ER + pR) * uR - d3);
 }
 
+// Solver on the reconstructed states (normal frame): HLLC, or with RS 1 / 2
+// carb_fv's HLL / Roe.  Branch-free, so its chain can interleave with the
+// HLLE chain where both are evaluated together.
 template <class R, int RS = 0>
-__device__ __forceinline__ void face_flux_fast(const R L[4], const R Rv[4], const R WL[4], const R WR[4], R cWL,
-                                               R cWR, R EWL, R EWR, const GasF<R> &gs, R F[4])
+__device__ __forceinline__ void recon_flux_fast(const R L[4], const R Rv[4], const GasF<R> &gs, R Fh[4])
 {
     const R zero = R(0);
-    // --- solver on the reconstructed states (branch-free, so its chain and
-    // the HLLE chain share one basic block and interleave) ---
-    R Fh0, Fh1, Fh2, Fh3;
     if constexpr (RS == 1 || RS == 2) {
-        R Fh[4];
         if constexpr (RS == 1) hll_fast<R>(L, Rv, gs, Fh);
         else roe_fast<R>(L, Rv, gs, Fh);
-        Fh0 = Fh[0]; Fh1 = Fh[1]; Fh2 = Fh[2]; Fh3 = Fh[3];
     } else {
         const R rL = L[0], uL = L[1], tL = L[2], pL = L[3];
         const R rR = Rv[0], uR = Rv[1], tR = Rv[2], pR = Rv[3];
@@ -421,50 +428,68 @@ __device__ __forceinline__ void face_flux_fast(const R L[4], const R Rv[4], cons
         const R q = sup ? zero : frcp(SK - Ss);
         const R fact = dK * q;
         const R m = rK * uK;
-        Fh0 = m + SKw * (fact - rK);
-        Fh1 = m * uK + pK + SKw * (fact * Ss - m);
-        Fh2 = Fh0 * tK;
-        Fh3 = (EK + pK) * uK + SKw * (q * (EK * (SK - uK) + (Ss - uK) * (dK * Ss + pK)) - EK);
+        Fh[0] = m + SKw * (fact - rK);
+        Fh[1] = m * uK + pK + SKw * (fact * Ss - m);
+        Fh[2] = Fh[0] * tK;
+        Fh[3] = (EK + pK) * uK + SKw * (q * (EK * (SK - uK) + (Ss - uK) * (dK * Ss + pK)) - EK);
     }
-    // --- HLLE of the cell states, and the pressure-jump sensor ---
-    R Fl0, Fl1, Fl2, Fl3, sd;
-    {
-        const R rL = WL[0], uL = WL[1], tL = WL[2], pL = WL[3];
-        const R rR = WR[0], uR = WR[1], tR = WR[2], pR = WR[3];
-        // Einfeldt's form: with SL- = min(SL, 0), SR+ = max(SR, 0) the HLL
-        // average equals FL, FR or the subsonic average in the three wave
-        // configurations, with no selects
-        const R SL = dmin<R>(dmin<R>(uL - cWL, uR - cWR), zero), SR = dmax<R>(dmax<R>(uL + cWL, uR + cWR), zero);
-        const R mL = rL * uL, mR = rR * uR;
-        const R FL1 = mL * uL + pL, FR1 = mR * uR + pR;
-        const R FL2 = mL * tL, FR2 = mR * tR;
-        const R FL3 = (EWL + pL) * uL, FR3 = (EWR + pR) * uR;
-        const R dS = dmax<R>(SR - SL, FVB_LIT(R, 1e-10));
-        const R dp = WR[3] - WL[3], ps = WR[3] + WL[3];
-        const R dp2 = dp * dp;
-        const R dd = dp2 + FVB_LIT(R, 0.1) * ps * ps;
-        R idS;
-        if constexpr (sizeof(R) == 8) {
-            // one FP64 reciprocal for the HLLE span and the sensor's
-            // denominator (dS >= 1e-10, dd >= 4e-29: the product is normal)
-            const R ip = frcp(dS * dd);
-            idS = dd * ip;
-            sd = dp2 * (dS * ip);
-        } else {
-            idS = frcp(dS);
-            sd = dp2 * frcp(dd);
-        }
-        const R SRL = SR * SL;
-        Fl0 = (SR * mL - SL * mR + SRL * (rR - rL)) * idS;
-        Fl1 = (SR * FL1 - SL * FR1 + SRL * (mR - mL)) * idS;
-        Fl2 = (SR * FL2 - SL * FR2 + SRL * (rR * tR - rL * tL)) * idS;
-        Fl3 = (SR * FL3 - SL * FR3 + SRL * (EWR - EWL)) * idS;
+}
+
+// HLLE of the two cell states (sound speeds cWL, cWR, energies EWL, EWR) and
+// the pressure-jump sensor s of the face, normal frame.
+template <class R>
+__device__ __forceinline__ void hlle_sensor_fast(const R WL[4], const R WR[4], R cWL, R cWR, R EWL, R EWR, R Fl[4],
+                                                 R &sd)
+{
+    const R zero = R(0);
+    const R rL = WL[0], uL = WL[1], tL = WL[2], pL = WL[3];
+    const R rR = WR[0], uR = WR[1], tR = WR[2], pR = WR[3];
+    // Einfeldt's form: with SL- = min(SL, 0), SR+ = max(SR, 0) the HLL
+    // average equals FL, FR or the subsonic average in the three wave
+    // configurations, with no selects
+    const R SL = dmin<R>(dmin<R>(uL - cWL, uR - cWR), zero), SR = dmax<R>(dmax<R>(uL + cWL, uR + cWR), zero);
+    const R mL = rL * uL, mR = rR * uR;
+    const R FL1 = mL * uL + pL, FR1 = mR * uR + pR;
+    const R FL2 = mL * tL, FR2 = mR * tR;
+    const R FL3 = (EWL + pL) * uL, FR3 = (EWR + pR) * uR;
+    const R dS = dmax<R>(SR - SL, FVB_LIT(R, 1e-10));
+    const R dp = WR[3] - WL[3], ps = WR[3] + WL[3];
+    const R dp2 = dp * dp;
+    const R dd = dp2 + FVB_LIT(R, 0.1) * ps * ps;
+    R idS;
+    if constexpr (sizeof(R) == 8) {
+        // one FP64 reciprocal for the HLLE span and the sensor's
+        // denominator (dS >= 1e-10, dd >= 4e-29: the product is normal)
+        const R ip = frcp(dS * dd);
+        idS = dd * ip;
+        sd = dp2 * (dS * ip);
+    } else {
+        idS = frcp(dS);
+        sd = dp2 * frcp(dd);
     }
-    // --- Ducros blend: (1 - s) Fh + s Fl ---
-    F[0] = Fh0 + sd * (Fl0 - Fh0);
-    F[1] = Fh1 + sd * (Fl1 - Fh1);
-    F[2] = Fh2 + sd * (Fl2 - Fh2);
-    F[3] = Fh3 + sd * (Fl3 - Fh3);
+    const R SRL = SR * SL;
+    Fl[0] = (SR * mL - SL * mR + SRL * (rR - rL)) * idS;
+    Fl[1] = (SR * FL1 - SL * FR1 + SRL * (mR - mL)) * idS;
+    Fl[2] = (SR * FL2 - SL * FR2 + SRL * (rR * tR - rL * tL)) * idS;
+    Fl[3] = (SR * FL3 - SL * FR3 + SRL * (EWR - EWL)) * idS;
+}
+
+// Ducros blend (1 - s) Fh + s Fl
+template <class R>
+__device__ __forceinline__ void ducros_blend(const R Fh[4], const R Fl[4], R sd, R F[4])
+{
+#pragma unroll
+    for (int q = 0; q < 4; ++q) F[q] = Fh[q] + sd * (Fl[q] - Fh[q]);
+}
+
+template <class R, int RS = 0>
+__device__ __forceinline__ void face_flux_fast(const R L[4], const R Rv[4], const R WL[4], const R WR[4], R cWL,
+                                               R cWR, R EWL, R EWR, const GasF<R> &gs, R F[4])
+{
+    R Fh[4], Fl[4], sd;
+    recon_flux_fast<R, RS>(L, Rv, gs, Fh);
+    hlle_sensor_fast<R>(WL, WR, cWL, cWR, EWL, EWR, Fl, sd);
+    ducros_blend<R>(Fh, Fl, sd, F);
 }
 
 }  // namespace fvb

@@ -21,6 +21,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -64,8 +65,8 @@ __device__ __forceinline__ void face_one(const R *W, int base, R *out, int ostri
         face_flux_fast<R, RS>(L, Rv, WL, WR, CE[-ST], CE[0], CE[PL - ST], CE[PL], gf, Fn);
     } else {
         R Fh[4], Fl[4];
-        hllc<R>(L, Rv, Fh, gs);
-        hlle<R>(WL, WR, Fl, gs);
+        hllc<R, !XDIR>(L, Rv, Fh, gs);
+        hlle<R, !XDIR>(WL, WR, Fl, gs);
         const R sd = ducros<R>(WL[3], WR[3]);
         const R one_m = R(1) - sd;
 #pragma unroll
@@ -227,6 +228,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
         }
         const R dt = R(ctl.dt);
         const R inv_h = R(1.0 / gd.h);
+        const R hR = R(gd.h);  // the FP32 form divides by h, as the shipped solver does
         // U0 of this thread's cells (stages 2 and 3), loaded now so the loads
         // are in flight while the faces are computed
         constexpr int CPT = (TX * TY + NT - 1) / NT;  // cells per thread
@@ -271,7 +273,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
             for (int q = 0; q < 4; ++q) {
                 const R *fx = FX + q * TY * (TX + 1) + r * (TX + 1) + c;
                 const R *fy = FY + q * (TY + 1) * TX + r * TX + c;
-                res[q] = -(fx[1] - fx[0]) * inv_h - (fy[TX] - fy[0]) * inv_h;
+                if constexpr (FAST) res[q] = -(fx[1] - fx[0]) * inv_h - (fy[TX] - fy[0]) * inv_h;
+                else res[q] = -(fx[1] - fx[0]) / hR - (fy[TX] - fy[0]) / hR;  // fv_up7_ducros_2d.cu:500-503
             }
             const int sc = (r + G) * SW + (c + G);
             if (a.stage == 0) {
@@ -354,7 +357,7 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
 
         // ---- 5. max wave speed of the new state (stage 3) ------------------
         if (a.stage == 3) {
-            // (a batched launch advances its grids' time in the stage-control kernel)
+            // (a batched launch advances each grid's time where its tile 0's header is published)
             if (!batched && tid == 0 && tile == 0) leader_finish<PREC>(gd.ctrl);
             if (batched) {
                 // tiles of one CTA belong to different grids: one atomic per
@@ -384,31 +387,6 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
     // a load still in flight after an error: wait for it (bounded) so no
     // copy into this CTA's shared memory outlives it
     if (s_err && gd_has_tma(a)) mbar_wait(&s_bar, phase);
-}
-
-// ---------------------------------------------------------------------------
-// step control of a batched launch, one thread per grid slot
-// ---------------------------------------------------------------------------
-template <int PREC>
-__global__ void stage_control_kernel(Ctrl *ctrl, int count, int stage, TileCtl *out)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
-    Ctrl *c = ctrl + i;
-    const TileCtl k = tile_control<PREC>(c, stage, true);
-    // the stage-3 tiles read only `active` and `dt`: the time advances here
-    if (stage == 3 && k.run) leader_finish<PREC>(c);
-    out[i] = k;
-}
-
-cudaError_t launch_stage_control(int prec, Ctrl *ctrl, int count, int stage, TileCtl *out, cudaStream_t s)
-{
-    if (count <= 0) return cudaSuccess;
-    const int nt = 128, nb = (count + nt - 1) / nt;
-    if (prec == P64) stage_control_kernel<P64><<<nb, nt, 0, s>>>(ctrl, count, stage, out);
-    else if (prec == P32) stage_control_kernel<P32><<<nb, nt, 0, s>>>(ctrl, count, stage, out);
-    else stage_control_kernel<P32C><<<nb, nt, 0, s>>>(ctrl, count, stage, out);
-    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -455,8 +433,21 @@ static KernelEntry entry32c(int shape)
     entry<P64, 7, 0, RS>(), entry<P64, 7, 1, RS>(), entry<P64, 7, 2, RS>(), entry<P64, 7, 3, RS>(), \
         entry<P64, 7, 4, RS>(), entry<P64, 7, 5, RS>()
 
+static KernelEntry entry64(int order, int shape, int rs)
+{
+    return KernelEntry{stage64_fn(order, shape, rs, false), stage64_fn(order, shape, rs, true),
+                       stage64_smem(order, shape), kTileShapes[shape].nt};
+}
+
 static KernelEntry *table_for(int prec, int order, int rs = 0)
 {
+    static const bool lean = [] {
+        const char *e = std::getenv("FVB_K64");
+        return !(e && e[0] == '1');
+    }();
+    static KernelEntry t64l_7[] = {entry64(7, 0, 0), entry64(7, 1, 0), entry64(7, 2, 0),
+                                   entry64(7, 3, 0), entry64(7, 4, 0), entry64(7, 5, 0)};
+    if (lean && prec == P64 && order == 7 && rs == 0) return t64l_7;
     static KernelEntry t64_7_hll[] = {FVB_SHAPES_RS(1)};
     static KernelEntry t64_7_roe[] = {FVB_SHAPES_RS(2)};
     if (rs != 0) return (prec == P64 && order == 7) ? (rs == 1 ? t64_7_hll : rs == 2 ? t64_7_roe : nullptr) : nullptr;

@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
 
         // ---- 5. max wave speed of the new state (stage 3) ------------------
         if (a.stage == 3) {
-            // (a batched launch advances its grids' time in the stage-control kernel)
+            // (a batched launch advances each grid's time where its tile 0's header is published)
             if (!batched && tid == 0 && tile == 0) leader_finish<P32C>(gd.ctrl);
             if (batched) {
                 // tiles of one CTA belong to different grids: one atomic per

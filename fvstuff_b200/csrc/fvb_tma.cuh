@@ -115,24 +115,27 @@ __device__ __forceinline__ void issue_tile_load(const GridDev &gd, int stage, in
 // Tile headers of a batched launch.  Warp 0 stages them one tile ahead:
 // the table entry of the CTA's next tile is loaded a tile early, and at the
 // top of each tile each lane of warp 0 loads one 8-byte word of the next
-// tile's grid descriptor or of its grid's step control for this stage
-// (written by the stage-control kernel before the launch), so these loads
-// are in flight while the tile is converted.  After the conversion barrier
-// warp 0 stores the words into shared memory and lane 0 starts the next
-// halo-box load; every thread reads the header after the barrier that ends
-// the tile.  (A single-grid launch reads its grid from the kernel parameter
-// and evaluates the step control once: it is the same for every tile.)
+// tile's grid descriptor or of its grid's step control (Ctrl), so these
+// loads are in flight while the tile is converted.  After the conversion
+// barrier warp 0 stores the words into shared memory, lane 0 evaluates the
+// stage's step control of that grid from the copy (the lane that publishes a
+// grid's tile 0 is that grid's leader and makes the stage's control writes,
+// including the time advance of stage 3) and starts the next halo-box load;
+// every thread reads the header after the barrier that ends the tile.  So a
+// batched stage needs no separate step-control launch.  (A single-grid
+// launch reads its grid from the kernel parameter and evaluates the step
+// control once: it is the same for every tile.)
 struct TileHdr {
     GridDev gd;
+    Ctrl c;
     TileCtl ctl;
     int tile;
     int pad;
 };
 constexpr int kGridWords = (int)(sizeof(GridDev) / 8);
-constexpr int kHdrWords = kGridWords + (int)(sizeof(TileCtl) / 8);
-static_assert(sizeof(GridDev) % 8 == 0 && sizeof(TileCtl) % 8 == 0 && kHdrWords <= 32,
-              "one warp copies a header");
-static_assert(offsetof(TileHdr, ctl) == sizeof(GridDev), "grid descriptor and step control are contiguous");
+constexpr int kHdrWords = kGridWords + (int)(sizeof(Ctrl) / 8);
+static_assert(sizeof(GridDev) % 8 == 0 && sizeof(Ctrl) % 8 == 0 && kHdrWords <= 32, "one warp copies a header");
+static_assert(offsetof(TileHdr, c) == sizeof(GridDev), "grid descriptor and step control are contiguous");
 
 // the grid of the current tile: its header in shared memory (batched) or
 // the kernel parameter (single grid); a reference, so each field is read
@@ -147,11 +150,12 @@ __device__ __forceinline__ const GridDev &tile_grid(const TileHdr &h, const Stag
 __device__ __forceinline__ unsigned long long hdr_word(const StageArgs &a, TileRef r, int lane)
 {
     if (lane < kGridWords) return reinterpret_cast<const unsigned long long *>(a.grids + r.grid)[lane];
-    if (lane < kHdrWords) return reinterpret_cast<const unsigned long long *>(a.ctls + r.grid)[lane - kGridWords];
+    if (lane < kHdrWords) return reinterpret_cast<const unsigned long long *>(a.ctrls + r.grid)[lane - kGridWords];
     return 0ull;
 }
 
-// warp 0: publish the header of tile r into h and start its halo-box load
+// warp 0: publish the header of tile r into h, evaluate its grid's step
+// control for this stage, and start its halo-box load
 template <int PREC, int G, int SW, int SH, int NT, class R>
 __device__ __forceinline__ void start_batched_tile(const StageArgs &a, TileHdr *h, TileRef r, unsigned long long w,
                                                    int parity, R *IN, uint64_t *bar, int lane)
@@ -160,6 +164,10 @@ __device__ __forceinline__ void start_batched_tile(const StageArgs &a, TileHdr *
     __syncwarp();
     if (lane == 0) {
         h->tile = r.tile;
+        Ctrl *ctrl = a.ctrls + r.grid;
+        const bool leader = r.tile == 0;
+        h->ctl = step_control<PREC>(h->c, ctrl, a.stage, leader);
+        if (a.stage == 3 && leader && h->ctl.run) leader_finish_from<PREC>(h->c, ctrl);
         if (h->gd.tmap) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             issue_tile_load<PREC, G, SW, SH, NT>(h->gd, a.stage, parity, r.tile, IN, bar, 0);
@@ -169,7 +177,7 @@ __device__ __forceinline__ void start_batched_tile(const StageArgs &a, TileHdr *
             mbar_arrive(bar);
             h->ctl.run = 0;
             h->ctl.copy = 0;
-            if (r.tile == 0) h->gd.ctrl->status = FVB_ERR_INVALID;
+            if (r.tile == 0) ctrl->status = FVB_ERR_INVALID;
         }
     }
     __syncwarp();
