@@ -72,6 +72,7 @@ SERVE_POLICY = {"fifo": 0, "shortest": 1}
 _P = C.c_void_p
 _SIG = {
     "fvb_version": (C.c_char_p, []),
+    "fvb_device_name": (C.c_char_p, [C.c_int]),
     "fvb_last_error": (C.c_char_p, []),
     "fvb_config_default": (None, [C.POINTER(Config), C.c_int]),
     "fvb_case_default": (None, [C.POINTER(Case), C.c_int, C.c_double, C.c_double, C.c_double]),

@@ -14,40 +14,14 @@
 #include <string>
 #include <vector>
 
+#include "fvb_cmaps.h"
+
 namespace fvbio {
 
 struct RGB {
     unsigned char r, g, b;
 };
 
-// Perceptual colormaps from their published nine-stop hex anchors,
-// interpolated linearly in RGB (the reference embeds matplotlib's 256-entry
-// tables; these agree with them to a few levels per channel).
-inline RGB stops9(const unsigned s[9], float t)
-{
-    float x = t * 8.0f;
-    int k = (int)x;
-    if (k >= 8) k = 7;
-    if (k < 0) k = 0;
-    float f = x - k;
-    auto ch = [&](int sh) {
-        float a = (float)((s[k] >> sh) & 255), b = (float)((s[k + 1] >> sh) & 255);
-        return (unsigned char)(a + (b - a) * f + 0.5f);
-    };
-    return RGB{ch(16), ch(8), ch(0)};
-}
-inline RGB viridis(float t)
-{
-    static const unsigned s[9] = {0x440154, 0x472d7b, 0x3b528b, 0x2c728e, 0x21918c,
-                                  0x28ae80, 0x5ec962, 0xaddc30, 0xfde725};
-    return stops9(s, t);
-}
-inline RGB plasma(float t)
-{
-    static const unsigned s[9] = {0x0d0887, 0x4c02a1, 0x7e03a8, 0xa92395, 0xcc4778,
-                                  0xe56b5d, 0xf89540, 0xfdc527, 0xf0f921};
-    return stops9(s, t);
-}
 // black -> red -> yellow -> white                  fv_up7_ducros_2d.cu:750-755
 inline RGB hot(float t)
 {
@@ -80,14 +54,16 @@ inline float unit(float v, float lo, float hi)
     return t;
 }
 
+// t in [0, 1] -> colour: the 256-level tables index floor(255 t), the
+// analytic maps take t itself                  fv_up7_ducros_2d.cu:869-876
 inline RGB color(int cmap, float t)
 {
     if (cmap == PLASMA || cmap == VIRIDIS) {
         int idx = (int)(t * 255.0f);
         if (idx < 0) idx = 0;
         if (idx > 255) idx = 255;
-        float ti = idx / 255.0f;
-        return cmap == PLASMA ? plasma(ti) : viridis(ti);
+        const unsigned char *e = cmap == PLASMA ? kPlasma[idx] : kViridis[idx];
+        return RGB{e[0], e[1], e[2]};
     }
     return cmap == HOT ? hot(t) : bwr(t);
 }

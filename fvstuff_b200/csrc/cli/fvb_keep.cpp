@@ -80,7 +80,8 @@ int main(int argc, char **argv)
     fvb_solver *s = nullptr;
     if (fvb_create(&cfg, &s)) { std::fprintf(stderr, "fvb_create: %s\n", fvb_last_error()); return 1; }
     std::printf("========================================================\n");
-    std::printf("  Device : %s\n", fvb_version());
+    const char *dev_name = fvb_device_name(cfg.device);
+    std::printf("  Device : %s\n", dev_name ? dev_name : fvb_version());
     std::printf("  Collocated FV + KEEP (ECKEP+ES, eq.41)  --  %s\n", lmv ? "Low-Mach Vortex" : "Circular Sod");
     if (lmv) std::printf("  eps=%.4f  (p0=%.3f)\n", eps, 1. / (gam * eps * eps) - 0.5);
     std::printf("  N=%dx%d  Np=%d  h=%.5f  CFL=%.2f  t_end=%.4f\n", N, N, N + 4, h, cfl, t_end);
@@ -141,7 +142,9 @@ int main(int argc, char **argv)
     const auto t0 = std::chrono::steady_clock::now();
     while (st.t < t_end) {
         if (fvb_step(s, 50, std::min(t_next, t_end)) || fvb_sync(s, &st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }
-        if (st.status) { std::fprintf(stderr, st.status == FVB_ERR_BLOWUP ? "NaN lam at step %lld\n" : "dt underflow at step %lld\n", (long long)st.steps); break; }
+        // the reference's two stops               keep_fv_euler_2d.cu:701-705
+        if (st.status == FVB_ERR_BLOWUP) { std::fprintf(stderr, "NaN lam at step %lld\n", (long long)st.steps); break; }
+        if (st.status) { std::fprintf(stderr, "dt underflow\n"); break; }
         if (st.t >= t_next - 1e-12 && f <= NF) {
             const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             std::printf("  frame %2d/%d  step %5lld  t=%.5f  lam=%.3e  elapsed=%.1fs\n", f, NF, (long long)st.steps, st.t,
@@ -156,9 +159,14 @@ int main(int argc, char **argv)
         fvb_get_state(s, Q.data(), FVB_LAYOUT_CONS, FVB_F64, FVB_HOST, 0);
         double er, ep;
         lmv_errors(Q, N, h, eps, gam, er, ep);
-        std::printf("  -- FINAL L2 ERRORS (Low-Mach Vortex) --\n");
+        // the reference's report block             keep_fv_euler_2d.cu:739-747
+        std::printf("  \u2500\u2500 FINAL L2 ERRORS (Low-Mach Vortex) "
+                    "\u2500\u2500\u2500\u2500\u2500\u2500\u2500\u2500\u2500\u2500\u2500\u2500\u2500\u2500\u2500\u2500\n");
         std::printf("  eps=%.4f  N=%d  h=%.5f  t=%.4f\n", eps, N, h, st.t);
         std::printf("  L2(rho) = %.6e\n  L2(p)   = %.6e\n", er, ep);
+        std::printf("  ");
+        for (int k = 0; k < 53; ++k) std::printf("\u2500");
+        std::printf("\n");
     }
     const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     std::printf("  Done: %lld steps  t=%.6f  wall=%.2fs\n", (long long)st.steps, st.t, wall);

@@ -170,7 +170,8 @@ int main(int argc, char **argv)
     const double h = cfg.length / a.n;
     static const char *names[] = {"Circular Sod", "Isentropic vortex", "Kelvin-Helmholtz", "Four-quadrant Riemann"};
     std::printf("========================================================\n");
-    std::printf("  Device  : %s\n", fvb_version());
+    const char *dev_name = fvb_device_name(cfg.device);
+    std::printf("  Device  : %s\n", dev_name ? dev_name : fvb_version());
     std::printf("  UP%d+HLLC+Ducros FV 2D  --  %s\n", a.order, names[a.kase]);
     if (a.d2av)
         std::printf("  n=%dx%d  h=%.5f  C2=%.3f  Cg=%.4f  sc=%.4f  CFL=%.2f  order=%d\n", a.n, a.n, h, a.c2, a.cg, a.sc,
@@ -238,10 +239,16 @@ int main(int argc, char **argv)
         enqueued = false;
         if (fvb_sync(s, &st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }
         if (st.status) {
-            std::fprintf(stderr, "  %s at step %lld t=%.6f lam_max=%.3e -- writing blow-up frame\n",
-                         st.status == FVB_ERR_BLOWUP ? "NaN/Inf lam_max" : "dt underflow", (long long)st.steps, st.t,
-                         st.lam_max);
-            write_frame_now(s, F, a, 99);
+            // the reference's two stops: a non-positive or NaN wave-speed
+            // maximum after a step (no frame), and a dt below 1e-14 (frame 99)
+            //                                   fv_up7_ducros_2d.cu:1002-1007, :1030
+            if (st.status == FVB_ERR_BLOWUP) {
+                std::fprintf(stderr, "blow-up after step %lld t=%.5f\n", (long long)st.steps, st.t);
+            } else {
+                std::fprintf(stderr, "  dt underflow at step %lld t=%.6f lam_max=%.3e \u2014 writing blow-up frame\n",
+                             (long long)st.steps, st.t, st.lam_max);
+                write_frame_now(s, F, a, 99);
+            }
             metric(st.status == FVB_ERR_BLOWUP ? "blowup" : "dt_underflow", st);
             break;
         }

@@ -285,6 +285,19 @@ extern "C" {
 
 const char *fvb_version(void) { return "fvb 0.1 (sm_100a)"; }
 
+const char *fvb_device_name(int device)
+{
+    thread_local std::string name;
+    cudaDeviceProp prop;
+    const cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) {
+        cuda_fail(e, "cudaGetDeviceProperties");
+        return nullptr;
+    }
+    name = prop.name;
+    return name.c_str();
+}
+
 const char *fvb_last_error(void) { return g_err.c_str(); }
 
 void fvb_config_default(fvb_config *c, int n)
@@ -467,10 +480,14 @@ fvb_status fvb_init_case(fvb_solver *s, const fvb_case *c)
     }
     fvb_status st = ensure_staging(s);
     if (st) return st;
-    cudaError_t e = init_case_prim64((double *)s->staging, s->n, s->cfg.x0, s->cfg.y0, s->gd.h, s->cfg.gamma, *c,
-                                     s->stream);
+    // the FP32 form as shipped starts its Sod from the FP32 evaluation
+    const bool sod32 = s->prec == P32 && c->kind == FVB_CASE_SOD;
+    cudaError_t e = sod32 ? init_sod_prim32((float *)s->staging, s->n, s->cfg.x0, s->cfg.y0, s->cfg.length, *c,
+                                            s->stream)
+                          : init_case_prim64((double *)s->staging, s->n, s->cfg.x0, s->cfg.y0, s->gd.h,
+                                             s->cfg.gamma, *c, s->stream);
     if (e != cudaSuccess) return cuda_fail(e, "initial state");
-    ExtView ev{1, s->g, s->G.np, FVB_LAYOUT_PRIM, FVB_F64};
+    ExtView ev{1, s->g, s->G.np, FVB_LAYOUT_PRIM, sod32 ? FVB_F32 : FVB_F64};
     int p = s->parity;
     e = import_state(s->staging, ev, s->gd.st[s->internal == INT_CONS_HILO ? p : 0], s->gd.lo[p], view_of(s->gd),
                      s->internal, s->cfg.gamma, s->stream);

@@ -183,6 +183,41 @@ __global__ void ic_kernel(double *out, int n, double x0, double y0, double h, do
     }
 }
 
+// The circular Sod state of the FP32 form as shipped, evaluated in FP32 in
+// the reference's expression order (fv_up7_ducros_2d.cu:618-639): FP32 h,
+// cell centres, radius, tanhf blend, so the initial state has the bits the
+// shipped solver starts from.  (4, n, n) floats, primitives.
+__global__ void ic_sod32_kernel(float *out, int n, float x0, float y0, float h, float xc0, float yc0, float rad,
+                                float r_out, float dr, float p_out, float dp)
+{
+    const long long n2 = (long long)n * n;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
+         k += (long long)blockDim.x * gridDim.x) {
+        const int j = (int)(k / n), i = (int)(k % n);
+        const float xc = x0 + (i + 0.5f) * h, yc = y0 + (j + 0.5f) * h;
+        const float r = sqrtf((xc - xc0) * (xc - xc0) + (yc - yc0) * (yc - yc0));
+        const float delta = 1.0f * h;
+        const float phi = 0.5f * (1.f + tanhf((rad - r) / delta));
+        out[k] = r_out + dr * phi;
+        out[n2 + k] = 0.f;
+        out[2 * n2 + k] = 0.f;
+        out[3 * n2 + k] = p_out + dp * phi;
+    }
+}
+
+cudaError_t init_sod_prim32(float *out, int n, double x0, double y0, double length, const fvb_case &c,
+                            cudaStream_t s)
+{
+    int blocks = (int)(((long long)n * n + 255) / 256);
+    if (blocks > 8192) blocks = 8192;
+    // h = 1.0f / N as the shipped solver forms it (scaled by the length)
+    const float h = (float)length * (1.0f / (float)n);
+    ic_sod32_kernel<<<blocks, 256, 0, s>>>(out, n, (float)x0, (float)y0, h, (float)c.param[0], (float)c.param[1],
+                                           (float)c.param[2], (float)c.param[3], (float)(c.param[4] - c.param[3]),
+                                           (float)c.param[5], (float)(c.param[6] - c.param[5]));
+    return cudaGetLastError();
+}
+
 cudaError_t init_case_prim64(double *out, int n, double x0, double y0, double h, double gam,
                              const fvb_case &c, cudaStream_t s)
 {
@@ -553,10 +588,17 @@ __global__ void frame_kernel(const float *Q, int n, int g, int np, float h, floa
         const float sy = fmaxf(frame_ducros(p, at(3, jp + 1, ip)), frame_ducros(at(3, jp - 1, ip), p));
         float w = 0.0f;
         if (g >= 3) {
-            const float dvdx = -at(2, jp, ip - 3) + 9.0f * at(2, jp, ip - 2) - 45.0f * at(2, jp, ip - 1) +
-                               45.0f * at(2, jp, ip + 1) - 9.0f * at(2, jp, ip + 2) + at(2, jp, ip + 3);
-            const float dudy = -at(1, jp - 3, ip) + 9.0f * at(1, jp - 2, ip) - 45.0f * at(1, jp - 1, ip) +
-                               45.0f * at(1, jp + 1, ip) - 9.0f * at(1, jp + 2, ip) + at(1, jp + 3, ip);
+            // the six taps (-1, 9, -45, 45, -9, 1)/60 accumulated one fused
+            // multiply-add at a time from zero, offset -3 first: the rounding
+            // of the reference's loop                fv_up7_ducros_2d.cu:812-820
+            const float cf[6] = {-1.f, 9.f, -45.f, 45.f, -9.f, 1.f};
+            const int off[6] = {-3, -2, -1, 1, 2, 3};
+            float dvdx = 0.f, dudy = 0.f;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) {
+                dvdx = fmaf(cf[d], at(2, jp, ip + off[d]), dvdx);
+                dudy = fmaf(cf[d], at(1, jp + off[d], ip), dudy);
+            }
             w = (dvdx - dudy) / (60.0f * h);
         } else {
             // two ghost layers (KEEP, rec3): the 4th-order central difference
@@ -570,7 +612,7 @@ __global__ void frame_kernel(const float *Q, int n, int g, int np, float h, floa
         out[k] = at(0, jp, ip);
         out[nn + k] = w;
         out[2 * nn + k] = fmaxf(sx, sy);
-        out[3 * nn + k] = sqrtf(u * u + v * v);
+        out[3 * nn + k] = sqrtf(fmaf(u, u, v * v));
         out[4 * nn + k] = p;
     }
 }

@@ -31,6 +31,9 @@ enum { INT_PRIM64 = 0, INT_PRIM32 = 1, INT_CONS_HILO = 2, INT_CONS64 = 3 };
 
 template <class R>
 cudaError_t bc_fill(R *buf, const BufView &v, int bcx, int bcy, cudaStream_t s);
+// circular Sod evaluated in FP32 as the shipped FP32 solver does (the FP32 form's initial state)
+cudaError_t init_sod_prim32(float *out, int n, double x0, double y0, double length, const fvb_case &c,
+                            cudaStream_t s);
 cudaError_t init_case_prim64(double *out, int n, double x0, double y0, double h, double gam, const fvb_case &c,
                              cudaStream_t s);
 cudaError_t import_state(const void *src, const ExtView &e, void *dst, void *dst_lo, const BufView &v,

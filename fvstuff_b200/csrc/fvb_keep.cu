@@ -55,6 +55,14 @@ __device__ __forceinline__ void k_evars(const double W[4], double s, double gam,
 // VL, VR: the two cells' entropy variables in the face frame (the Cartesian
 // ones of k_evars with (u, v) -> (un, ut): for the normals (1, 0) and (0, 1)
 // a relabelling and one exact negation, so the values are the reference's)
+//
+// The steps and their association order are the published flux's as the
+// reference evaluates them (the ECKEP averages, the MOVERS-RH coefficient
+// with its division by dV3^2 + 1e-16 and the sonic fix), not a rewrite:
+// where dV3 is small that division amplifies a last-bit difference in its
+// operands by many orders of magnitude, so any reassociation here moves the
+// low-Mach vortex run outside the spread between the reference's own GPU
+// and host builds, which is the tolerance this family is held to.
 __device__ __forceinline__ void k_flux(const double WL[4], const double WR[4], const double VL[4],
                                        const double VR[4], double nx, double ny, double gam, double Fec[4],
                                        double *alphaS)

@@ -133,6 +133,9 @@ typedef struct fvb_stats {
 typedef struct fvb_solver fvb_solver;
 
 FVB_API const char *fvb_version(void);
+/* name of CUDA device `device` (valid until the next call on this thread),
+ * or NULL with the error set       the "Device" line, fv_up7_ducros_2d.cu:894-898 */
+FVB_API const char *fvb_device_name(int device);
 /* text of the last error on this thread */
 FVB_API const char *fvb_last_error(void);
 /* default configuration: UP7 + Ducros, FP64, reflecting walls, [0,1]^2,

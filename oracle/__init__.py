@@ -562,3 +562,31 @@ def refg_program(kind: str, args: list[str]) -> list[str]:
             "ctypes.CDLL(None).fflush(None)\n"
             "sys.exit(r)\n")
     return [sys.executable, "-c", code, lib_path, *args]
+
+
+def refg_up7_frame(Q: np.ndarray, N: int, h: float, fn: str) -> None:
+    """The reference's frame pipeline (its sensor and derived-field kernels,
+    colour ranges and 2x2 composite writer) on the padded primitive state Q
+    (float32 as shipped, or float64 with the retype), written to `fn`."""
+    s = _sfx(Q.dtype)
+    st = getattr(ref_gpu("up7_" + s), "refg_up7_frame_" + s)(_ptr(np.ascontiguousarray(Q)), C.c_int(N),
+                                                             _real(Q.dtype)(h), str(fn).encode())
+    if st != 0:
+        raise RuntimeError("reference frame failed: cuda error %d" % st)
+
+
+def refg_program(kind: str, args: list[str]) -> list[str]:
+    """Command line that runs the reference program itself -- its main(),
+    unchanged, from the GPU build of `kind` ('up7_f32', 'keep', ...) -- with
+    `args`, in a process of its own (it writes its files into the current
+    directory and its report to stdout)."""
+    import sys
+    lib_path = str(REF / ("libref_gpu_%s.so" % kind))
+    code = ("import ctypes, sys\n"
+            "L = ctypes.CDLL(sys.argv[1])\n"
+            "argv = [b'ref'] + [a.encode() for a in sys.argv[2:]]\n"
+            "arr = (ctypes.c_char_p * len(argv))(*argv)\n"
+            "r = L.refg_main(len(argv), arr)\n"
+            "ctypes.CDLL(None).fflush(None)\n"
+            "sys.exit(r)\n")
+    return [sys.executable, "-c", code, lib_path, *args]

@@ -4,7 +4,7 @@
  * GPU build of the reference solvers' own CUDA kernels: the reference
  * source file itself is #included (REF_CU; the FP64 variant is the
  * float->double retype generated by oracle/build.py under oracle/_ref/),
- * with its main() renamed out of the way.  This file adds host-array entry
+ * with its main() renamed (and exported as refg_main).  This file adds host-array entry
  * points that run the reference's kernels with the reference's launch
  * configuration and host loop, for the GPU parity tests and for timing the
  * reference kernels on the same device.
@@ -12,6 +12,11 @@
 #define main fvref_unused_main
 #include REF_CU
 #undef main
+
+/* the reference program itself: its main() unchanged (argument parsing,
+ * time loop, stdout lines and output files in the current directory), for
+ * the tests that compare the command-line drivers' outputs with it */
+extern "C" int refg_main(int argc, char **argv) { return fvref_unused_main(argc, argv); }
 
 #define CAT2(a, b) a##b
 #define CAT(a, b) CAT2(a, b)
@@ -54,6 +59,44 @@ static void bc_launch(R *d, int N, int Np, int bc)
 }
 
 extern "C" {
+
+/* the reference's frame of a padded primitive state Qh (host): its
+ * compute_sensor and compute_derived kernels, the colour ranges of its
+ * WRITE_FRAME (density 0.125 .. 10.1, vorticity symmetric about its largest
+ * magnitude, sensor 0 .. 1, |v| 0 .. its max) and its write_ppm_2x2
+ * (fv_up7_ducros_2d.cu:931-971, :835-881), into file `fn` */
+int API(refg_up7_frame_)(const R *Qh, int N, R h, const char *fn)
+{
+    const int Np = N + 2 * ORDER_G;
+    size_t nP = (size_t)4 * Np * Np, n1 = (size_t)N * N;
+    R *dQ = nullptr, *dSD = nullptr, *dW = nullptr, *dV = nullptr;
+    RET_ON_ERR(cudaMalloc(&dQ, nP * sizeof(R)));
+    RET_ON_ERR(cudaMalloc(&dSD, n1 * sizeof(R)));
+    RET_ON_ERR(cudaMalloc(&dW, n1 * sizeof(R)));
+    RET_ON_ERR(cudaMalloc(&dV, n1 * sizeof(R)));
+    RET_ON_ERR(cudaMemcpy(dQ, Qh, nP * sizeof(R), cudaMemcpyHostToDevice));
+    compute_sensor<<<GS_NBLK, BLOCK1D>>>(dQ, dSD, N, Np);
+    compute_derived<<<GS_NBLK, BLOCK1D>>>(dQ, dW, dV, N, Np, h);
+    RET_ON_ERR(cudaDeviceSynchronize());
+    R *rho = (R *)malloc(n1 * sizeof(R)), *sd = (R *)malloc(n1 * sizeof(R));
+    R *vort = (R *)malloc(n1 * sizeof(R)), *vmag = (R *)malloc(n1 * sizeof(R));
+    for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) rho[(size_t)j * N + i] = Qh[(size_t)(j + ORDER_G) * Np + i + ORDER_G];
+    RET_ON_ERR(cudaMemcpy(sd, dSD, n1 * sizeof(R), cudaMemcpyDeviceToHost));
+    RET_ON_ERR(cudaMemcpy(vort, dW, n1 * sizeof(R), cudaMemcpyDeviceToHost));
+    RET_ON_ERR(cudaMemcpy(vmag, dV, n1 * sizeof(R), cudaMemcpyDeviceToHost));
+    const R RHO_MIN = 0.125, RHO_MAX = 10.1;
+    R wmax = 1e-10f, vmax = 1e-10f;
+    for (size_t k = 0; k < n1; k++) {
+        R aw = vort[k] < 0.0 ? -vort[k] : vort[k];
+        if (aw > wmax) wmax = aw;
+        if (vmag[k] > vmax) vmax = vmag[k];
+    }
+    write_ppm_2x2(fn, rho, RHO_MIN, RHO_MAX, 0, vort, -wmax, wmax, 3, sd, 0.0, 1.0, 2, vmag, 0.0, vmax, 1, N);
+    free(rho); free(sd); free(vort); free(vmag);
+    cudaFree(dQ); cudaFree(dSD); cudaFree(dW); cudaFree(dV);
+    return 0;
+}
 
 /* one compute_rhs launch (fv_up7_ducros_2d.cu:370) on host arrays */
 int API(refg_up7_rhs_)(const R *Qh, R *RHSh, R *lamh, int N, int Np, R h)

@@ -1,0 +1,195 @@
+"""The drop-in's files and report against the reference programs themselves.
+
+The reference's own main() functions (fv_up7_ducros_2d.cu as shipped, FP32;
+keep_fv_euler_2d.cu, FP64), built unchanged for the GPU by the oracle's
+recipe, run beside the command-line drivers fvb_up7 --precision f32 and
+fvb_keep on the same grid, and their outputs are compared:
+
+* the composite PPM frames sod_%04d.ppm (fv_up7_ducros_2d.cu:835-881,
+  :931-971): byte for byte where the states are the same bits (the initial
+  frame, and any state handed to both frame pipelines), and pixel by pixel
+  over the whole run, where the two FP32 solvers may drift apart by a few ulp;
+* keep_fv's figures/keep_sod_%04d.png (keep_fv_euler_2d.cu:561-589,
+  :671-687) by decoded pixels (the compressed bytes differ: the reference
+  uses stb_image_write's filters and deflate, this writer stored blocks);
+* the stdout lines (fv_up7_ducros_2d.cu:897-902, :1036-1056;
+  keep_fv_euler_2d.cu:610-619, :722-757), with the wall-clock figures masked.
+"""
+from __future__ import annotations
+
+import re
+import subprocess
+import zlib
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import fvstuff_b200 as F
+import oracle as O
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (O.REF / "libref_gpu_up7_f32.so").exists(), reason="reference GPU build absent")]
+
+BIN = Path(F.__file__).resolve().parent / "bin"
+
+
+def _ppm(path):
+    raw = Path(path).read_bytes()
+    m = re.match(rb"P6\n(\d+) (\d+)\n255\n", raw)
+    w, h = int(m.group(1)), int(m.group(2))
+    return np.frombuffer(raw[m.end():], np.uint8).reshape(h, w, 3)
+
+
+def _png(path):
+    """RGB pixels of an 8-bit truecolour PNG (any filter types)."""
+    raw = Path(path).read_bytes()
+    assert raw[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat, w = 8, b"", None
+    while pos < len(raw):
+        n = int.from_bytes(raw[pos:pos + 4], "big")
+        kind, body = raw[pos + 4:pos + 8], raw[pos + 8:pos + 8 + n]
+        if kind == b"IHDR":
+            w, h = int.from_bytes(body[:4], "big"), int.from_bytes(body[4:8], "big")
+            assert body[8] == 8 and body[9] == 2
+        elif kind == b"IDAT":
+            idat += body
+        pos += 12 + n
+    data = zlib.decompress(idat)
+    stride, bpp = 3 * w, 3
+    out = np.zeros((h, stride), np.uint8)
+    prev = np.zeros(stride, np.int32)
+    for r in range(h):
+        f = data[r * (stride + 1)]
+        line = np.frombuffer(data[r * (stride + 1) + 1:(r + 1) * (stride + 1)], np.uint8).astype(np.int32)
+        cur = np.zeros(stride, np.int32)
+        for i in range(stride):
+            a = cur[i - bpp] if i >= bpp else 0
+            b = prev[i]
+            c = prev[i - bpp] if i >= bpp else 0
+            if f == 0:
+                p = 0
+            elif f == 1:
+                p = a
+            elif f == 2:
+                p = b
+            elif f == 3:
+                p = (a + b) // 2
+            else:
+                pa, pb, pc = abs(b - c), abs(a - c), abs(a + b - 2 * c)
+                p = a if pa <= pb and pa <= pc else (b if pb <= pc else c)
+            cur[i] = (line[i] + p) & 255
+        out[r] = cur
+        prev = cur
+    return out.reshape(h, w, 3)
+
+
+# wall-clock figures differ run to run; every other character must agree
+_CLOCK = re.compile(r"(elapsed=|wall=|ETA=)[0-9.]+")
+
+
+def _masked(text):
+    return [_CLOCK.sub(r"\1#", ln) for ln in text.splitlines()]
+
+
+def _run(cmd, cwd):
+    r = subprocess.run([str(c) for c in cmd], cwd=cwd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    return r
+
+
+@pytest.fixture(scope="module")
+def up7(tmp_path_factory):
+    n = 32
+    a, b = tmp_path_factory.mktemp("ref_up7"), tmp_path_factory.mktemp("fvb_up7")
+    ra = _run(O.refg_program("up7_f32", [str(n)]), a)
+    rb = _run([BIN / "fvb_up7", n, "--precision", "f32"], b)
+    return n, a, b, ra.stdout, rb.stdout
+
+
+def test_up7_initial_frame_is_byte_identical(up7):
+    n, a, b, _, _ = up7
+    ref, ours = (a / "sod_0000.ppm").read_bytes(), (b / "sod_0000.ppm").read_bytes()
+    assert len(ours) == len(ref) == len(b"P6\n64 64\n255\n") + 3 * (2 * n) ** 2
+    assert ours == ref
+
+
+def test_up7_frames_over_the_run(up7):
+    """Every frame of the run, pixel by pixel against the reference's."""
+    n, a, b, _, _ = up7
+    for k in range(11):
+        ref, ours = _ppm(a / ("sod_%04d.ppm" % k)), _ppm(b / ("sod_%04d.ppm" % k))
+        assert ref.shape == ours.shape == (2 * n, 2 * n, 3)
+        same = np.mean(np.all(ref == ours, axis=2))
+        print("frame %2d: %.4f of the pixels identical, largest channel difference %d"
+              % (k, same, int(np.max(np.abs(ref.astype(int) - ours.astype(int))))))
+        assert same >= 0.99, k
+
+
+def test_up7_stdout_matches_reference(up7):
+    _, _, _, ref, ours = up7
+    ra, rb = _masked(ref), _masked(ours)
+    diff = [(x, y) for x, y in zip(ra, rb) if x != y]
+    for x, y in diff:
+        print("reference: %r\nfvb:       %r" % (x, y))
+    assert len(ra) == len(rb)
+    # the banner, frame, progress, Saved and Done lines agree character for
+    # character (clock figures masked)
+    assert ra[:5] == rb[:5]
+    assert len(diff) <= 2
+
+
+def test_frame_pipeline_bytes_on_an_evolved_state(tmp_path):
+    """The same FP32 state through both frame pipelines -- the reference's
+    sensor and derived-field kernels and composite writer, and this library's
+    device frame extraction and the driver's writer -- gives the same bytes.
+    The state is the reference's own after 40 steps of its Sod (vorticity,
+    |v| and the sensor are all non-trivial there)."""
+    n = 48
+    h = np.float32(1.0 / n)
+    U = O.ref_up_ic_sod(n, 1.0 / n, np.float32)
+    O.ref_up_bc(U, n, 0)
+    O.refg_up_run(U, n, h, np.float32(0.4), 0, 40)
+    O.refg_up7_frame(U, n, h, str(tmp_path / "ref.ppm"))
+    s = F.Solver(n, precision="f32")
+    s.set_state(U)
+    s.save(tmp_path / "state.ckpt")
+    s.close()
+    _run([BIN / "fvb_up7", n, "--precision", "f32", "--resume", "state.ckpt", "--t-end", "1e-6", "--frames", "1",
+          "--prefix", "ours"], tmp_path)
+    assert (tmp_path / "ours_0000.ppm").read_bytes() == (tmp_path / "ref.ppm").read_bytes()
+
+
+@pytest.fixture(scope="module")
+def keep(tmp_path_factory):
+    n = 40
+    a, b = tmp_path_factory.mktemp("ref_keep"), tmp_path_factory.mktemp("fvb_keep")
+    (a / "figures").mkdir()
+    ra = _run(O.refg_program("keep", [str(n)]), a)
+    rb = _run([BIN / "fvb_keep", n], b)
+    return n, a, b, ra.stdout, rb.stdout
+
+
+def test_keep_png_pixels_match_reference(keep):
+    n, a, b, _, _ = keep
+    for k in range(11):
+        fn = "figures/keep_sod_%04d.png" % k
+        ref, ours = _png(a / fn), _png(b / fn)
+        assert ref.shape == ours.shape == (n, 2 * n, 3)
+        same = np.mean(np.all(ref == ours, axis=2))
+        print("keep frame %2d: %.4f of the pixels identical" % (k, same))
+        if k == 0:
+            assert np.array_equal(ref, ours)
+        else:
+            assert same >= 0.999, k
+
+
+def test_keep_stdout_matches_reference(keep):
+    _, _, _, ref, ours = keep
+    ra, rb = _masked(ref), _masked(ours)
+    for x, y in zip(ra, rb):
+        if x != y:
+            print("reference: %r\nfvb:       %r" % (x, y))
+    assert len(ra) == len(rb)
+    assert ra[:6] == rb[:6]
+    assert sum(x != y for x, y in zip(ra, rb)) <= 2
