@@ -3,8 +3,12 @@ of fv_up7_ducros_2d.cu (compute_rhs + rk3_sX + apply_bc + gpu_max, its D2D
 copy and per-step host sync), built from the reference source for sm_100a in
 FP32 as shipped and retyped to FP64, against this library on the same
 Kelvin-Helmholtz 2048^2 periodic grid, same dt rule, CUDA-event timed.
-Prints the table that the measurement notes quote; asserts only that the
-fused path is faster than the kernels it replaces."""
+Prints the table that the measurement notes quote; asserts that the fused
+path is faster than the kernels it replaces and that, after the same steps
+from the same state, the plain FP64 path matches the reference's FP64
+kernels within 1e-12 relative L-inf on the conserved variables (and the
+FP32 mode the shipped FP32 kernels within 1e-5), at the headline sizes
+2048^2 and 8192^2."""
 from __future__ import annotations
 
 import numpy as np
@@ -12,12 +16,30 @@ import pytest
 
 import fvstuff_b200 as F
 import oracle as O
-from cases import kh, pad, rel_linf
+from cases import kh, pad, prim_to_cons, rel_linf
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not O.have_ref_gpu(), reason="reference GPU build absent")]
 
 N, STEPS = 2048, 20
+TOL64, TOL32 = 1e-12, 1e-5
+
+
+def _cons(U, g=4):
+    n = U.shape[-1] - 2 * g
+    return prim_to_cons(U[:, g:g + n, g:g + n].astype(np.float64))
+
+
+def _ours_state(n, precision, U, steps):
+    """this library's state after `steps` steps from the padded state U"""
+    s = F.Solver(n, bc="periodic", cfl=0.5, precision=precision)
+    s.set_state(U)
+    s.step(steps)
+    st = s.sync()
+    got = s.get_state(dtype=np.float32 if precision == "f32" else np.float64)
+    s.close()
+    assert st.status == 0 and st.steps == steps
+    return got, st
 
 
 def _ours_ms(precision, U64):
@@ -44,13 +66,25 @@ def test_faster_than_reference_kernels_kh2048():
     O.bc(U64, N, 4, 1)
     rows = []
     ref = {}
+    final = {}
     for dtype, tag in ((np.float32, "reference kernels, FP32 as shipped"),
                        (np.float64, "reference kernels, FP64 retype")):
         U = U64.astype(dtype)
         status, t, k, lmax, dt, ms = O.refg_up_run(U, N, 1.0 / N, 0.5, 1, STEPS)
         assert status == 0 and k == STEPS
         ref[dtype] = ms / STEPS
+        final[dtype] = (U, t)
         rows.append((tag, ms / STEPS))
+    # parity on the headline configuration: the same 20 steps from the same state
+    got64, st64 = _ours_state(N, "f64", U64, STEPS)
+    err64 = rel_linf(_cons(got64), _cons(final[np.float64][0]))
+    got32, st32 = _ours_state(N, "f32", U64.astype(np.float32), STEPS)
+    err32 = rel_linf(_cons(got32), _cons(final[np.float32][0]))
+    print("\nKH %d^2, %d steps: rel L-inf vs reference kernels: FP64 %.3e, FP32 %.3e" % (N, STEPS, err64, err32))
+    assert abs(st64.t - final[np.float64][1]) <= 1e-13 * st64.t
+    assert err64 <= TOL64
+    assert err32 <= TOL32
+    del got64, got32, final
     ours = {p: _ours_ms(p, U64) for p in ("f64", "f32c", "f32")}
     rows += [("fvb FP64 (plain method)", ours["f64"]), ("fvb FP32-compensated", ours["f32c"]),
              ("fvb FP32 (reference rounding)", ours["f32"])]
@@ -97,8 +131,9 @@ def test_keep_faster_than_reference_kernels():
     assert ms < ms_ref
 
 
-def _ours_rate(n, precision, w, steps=None, t_stop=None, **kw):
-    """cell-stage updates/s of this library on a prepared primitive state"""
+def _ours_rate(n, precision, w, steps=None, t_stop=None, keep_state=False, **kw):
+    """cell-stage updates/s of this library on a prepared primitive state
+    (and, with keep_state, the padded state at the end of the timed steps)"""
     import torch
     stream = torch.cuda.Stream()
     s = F.Solver(n, bc="periodic", cfl=0.5, precision=precision, stream=stream.cuda_stream, **kw)
@@ -117,8 +152,10 @@ def _ours_rate(n, precision, w, steps=None, t_stop=None, **kw):
     e1.record(stream)
     torch.cuda.synchronize()
     st = s.sync()
+    got = s.get_state() if keep_state else None
     s.close()
-    return 3.0 * n * n * st.steps / (e0.elapsed_time(e1) / 1e3), st.steps
+    rate = 3.0 * n * n * st.steps / (e0.elapsed_time(e1) / 1e3)
+    return (rate, st.steps, got, st) if keep_state else (rate, st.steps)
 
 
 def test_baseline_table_configs_1_and_5():
@@ -156,15 +193,28 @@ def test_baseline_table_configs_1_and_5():
     U = pad(w, 4)
     O.bc(U, n, 4, 1)
     ref = {}
+    final64 = None
     for dtype, tag in ((np.float32, "B1 reference GPU, FP32"), (np.float64, "B2 reference GPU, FP64")):
-        st, t, k, lmax, dt, ms = O.refg_up_run(U.astype(dtype), n, 1.0 / n, 0.5, 1, steps)
+        V = U.astype(dtype)
+        st, t, k, lmax, dt, ms = O.refg_up_run(V, n, 1.0 / n, 0.5, 1, steps)
         assert st == 0 and k == steps
         ref[dtype] = 3.0 * n * n * steps / (ms / 1e3)
         rows.append(("5", tag, ref[dtype]))
+        if dtype == np.float64:
+            final64 = (_cons(V), t)
+        del V
     del U
-    for prec in ("f64", "f32c"):
-        r, _ = _ours_rate(n, prec, w, steps=steps)
-        rows.append(("5", "fvb " + prec, r))
+    r, _, got, st = _ours_rate(n, "f64", w, steps=steps, keep_state=True)
+    rows.append(("5", "fvb f64", r))
+    # parity on configuration 5's grid: the same 20 steps from the same state
+    err = rel_linf(_cons(got), final64[0])
+    del got
+    print("\nKH %d^2, %d steps: FP64 rel L-inf vs reference kernels %.3e" % (n, steps, err))
+    assert abs(st.t - final64[1]) <= 1e-13 * st.t
+    assert err <= TOL64
+    del final64
+    r, _ = _ours_rate(n, "f32c", w, steps=steps)
+    rows.append(("5", "fvb f32c", r))
     print("\nconfig  arm                              G cell-stages/s")
     for c, tag, r in rows:
         print("  %s     %-32s %9.4f" % (c, tag, r / 1e9))
