@@ -1,7 +1,7 @@
 // fvb_keep -- command-line drop-in for fvStuff's keep_fv (keep_fv_euler_2d.cu
 // main, :594-764) on libfvb.
 //
-//   fvb_keep [N] [lmv [eps]] [--cfl C] [--t-end T]
+//   fvb_keep [N] [lmv [eps]] [--cfl C] [--t-end T] [--resume FILE]
 //
 // Circular Sod (default) or the stationary low-Mach vortex with Mach number
 // eps (default 0.1) on the periodic unit square, KEEP flux (ECKEP + JST /
@@ -56,11 +56,13 @@ int main(int argc, char **argv)
     int N = 200;
     bool lmv = false;
     double eps = 0.1, cfl = 0.2, t_end = -1.0;
+    std::string resume;
     int pos = 0;
     for (int k = 1; k < argc; ++k) {
         std::string s = argv[k];
         if (s == "--cfl" && k + 1 < argc) cfl = std::atof(argv[++k]);
         else if (s == "--t-end" && k + 1 < argc) t_end = std::atof(argv[++k]);
+        else if (s == "--resume" && k + 1 < argc) resume = argv[++k];
         else if (pos == 0) { N = std::atoi(s.c_str()); ++pos; }
         else if (pos == 1) { lmv = (s == "lmv"); ++pos; }
         else if (pos == 2 && lmv) {
@@ -91,6 +93,11 @@ int main(int argc, char **argv)
     fvb_case_default(&c, lmv ? FVB_CASE_LMV : FVB_CASE_KEEP_SOD, 0, 0, 1);
     if (lmv) c.param[0] = eps;
     if (fvb_init_case(s, &c)) { std::fprintf(stderr, "init: %s\n", fvb_last_error()); return 1; }
+    // continue from a checkpoint (fvb_save) of a solver of this configuration
+    if (!resume.empty() && fvb_load(s, resume.c_str())) {
+        std::fprintf(stderr, "resume: %s\n", fvb_last_error());
+        return 1;
+    }
 
     const int Np = N + 4;
     std::vector<double> Q((size_t)4 * Np * Np);
@@ -133,12 +140,14 @@ int main(int argc, char **argv)
             std::printf("    L2_rho=%.4e  L2_p=%.4e\n", er, ep);
         }
     };
-    frame(0);
     const int NF = 10;
     int f = 1;
-    double t_next = t_end / NF;
     fvb_stats st;
     fvb_sync(s, &st);
+    // a resumed run starts at the first frame after its time
+    if (st.t == 0.0) frame(0);
+    else while (f <= NF && st.t >= f * t_end / NF - 1e-12) ++f;
+    double t_next = f * t_end / NF;
     const auto t0 = std::chrono::steady_clock::now();
     while (st.t < t_end) {
         if (fvb_step(s, 50, std::min(t_next, t_end)) || fvb_sync(s, &st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }

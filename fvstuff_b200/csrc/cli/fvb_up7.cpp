@@ -202,10 +202,17 @@ int main(int argc, char **argv)
     }
     fvb_stats st;
     fvb_sync(s, &st);
+    // frame times; the FP32 form keeps float time as the shipped solver does
+    // (float t_next = frame * t_end / N_FRAMES, fv_up7_ducros_2d.cu:983, :1050)
+    auto frame_time = [&](int f) {
+        return a.precision == FVB_PREC_F32 ? (double)((float)f * (float)a.t_end / (float)a.frames)
+                                           : f * a.t_end / a.frames;
+    };
+    const double t_end = a.precision == FVB_PREC_F32 ? (double)(float)a.t_end : a.t_end;
     int frame = 1;
     if (a.resume.empty() || st.t == 0.0) write_frame_now(s, F, a, 0);
-    else while (frame <= a.frames && st.t >= frame * a.t_end / a.frames - 1e-12) ++frame;
-    double t_next = frame * a.t_end / a.frames;
+    else while (frame <= a.frames && st.t >= frame_time(frame) - 1e-12) ++frame;
+    double t_next = frame_time(frame);
     const auto t0 = std::chrono::steady_clock::now();
     auto elapsed = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
     long long last_print = st.steps;
@@ -232,9 +239,9 @@ int main(int argc, char **argv)
     // at most 50 steps per call so progress prints like the reference's
     auto issue = [&](const fvb_stats &cur) {
         const int chunk = (int)(50 - (cur.steps % 50));
-        return fvb_step(s, chunk, std::min(t_next, a.t_end)) == FVB_OK;
+        return fvb_step(s, chunk, std::min(t_next, t_end)) == FVB_OK;
     };
-    while (st.t < a.t_end) {
+    while (st.t < t_end) {
         if (!enqueued && !issue(st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }
         enqueued = false;
         if (fvb_sync(s, &st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }
@@ -259,9 +266,9 @@ int main(int argc, char **argv)
             metric("frame", st);
             if (fvb_frame_begin(s)) { std::fprintf(stderr, "frame: %s\n", fvb_last_error()); return 1; }
             ++frame;
-            t_next = frame * a.t_end / a.frames;
+            t_next = frame_time(frame);
             // the next steps run on the GPU while this frame is written
-            if (st.t < a.t_end) {
+            if (st.t < t_end) {
                 if (!issue(st)) { std::fprintf(stderr, "%s\n", fvb_last_error()); return 1; }
                 enqueued = true;
             }
@@ -269,7 +276,7 @@ int main(int argc, char **argv)
         } else if (st.steps / 50 != last_print / 50) {
             const double el = elapsed();
             std::printf("  step %5lld  t=%.5f  dt=%.3e  elapsed=%.1fs  ETA=%.0fs\n", (long long)st.steps, st.t, st.dt,
-                        el, st.t > 0 ? (a.t_end - st.t) / st.t * el : 0.0);
+                        el, st.t > 0 ? (t_end - st.t) / st.t * el : 0.0);
             std::fflush(stdout);
         }
         last_print = st.steps;

@@ -801,7 +801,9 @@ fvb_status fvb_advance(fvb_solver *s, double t_stop, int64_t max_steps, int chun
         if (r) return r;
         if (st.status) return fail((fvb_status)st.status, "step control stopped at t=%.9g step %lld (%s)", st.t,
                                    (long long)st.steps, st.status == FVB_ERR_BLOWUP ? "lam_max not > 0" : "dt underflow");
-        if (!(st.t < t_stop) || done >= max_steps) return FVB_OK;
+        // (the FP32 form's time is a float: it stops at the float t_stop)
+        const bool before = s->prec == P32 ? (float)st.t < (float)t_stop : st.t < t_stop;
+        if (!before || done >= max_steps) return FVB_OK;
         int64_t k = chunk;
         if (k <= 0) {
             double dt = st.lam_max > 0 ? s->cfg.cfl * (s->cfg.length / s->n) / st.lam_max : 0;

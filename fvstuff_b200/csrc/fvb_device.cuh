@@ -141,7 +141,10 @@ __device__ TileCtl step_control(const Ctrl &s, Ctrl *c, int stage, bool leader)
     if (stage == 0) { k.run = 1; return k; }
     if (stage == 1) {
         double t = s.t, ts = s.t_stop;
-        if (s.status != 0 || !(t < ts)) {
+        // the FP32 form keeps float time, as the shipped solver does: a stop
+        // time is reached when the float time reaches its float value
+        const bool reached = PREC == P32 ? !((float)t < (float)ts) : !(t < ts);
+        if (s.status != 0 || reached) {
             if (leader) c->active = 0;
             return k;
         }

@@ -590,3 +590,12 @@ def refg_program(kind: str, args: list[str]) -> list[str]:
             "ctypes.CDLL(None).fflush(None)\n"
             "sys.exit(r)\n")
     return [sys.executable, "-c", code, lib_path, *args]
+
+
+def refg_keep_frame(Q: np.ndarray, N: int, lmv: bool, fn: str) -> None:
+    """The reference's KEEP frame pipeline (its extract_fields kernel, colour
+    ranges and 2-panel PNG writer) on the padded conserved state Q (g = 2)."""
+    st = ref_gpu("keep").refg_keep_frame(_ptr(np.ascontiguousarray(Q, dtype=np.float64)), C.c_int(N),
+                                         C.c_int(int(lmv)), str(fn).encode())
+    if st != 0:
+        raise RuntimeError("reference frame failed: cuda error %d" % st)

@@ -180,6 +180,35 @@ typedef double R;
 
 extern "C" {
 
+/* the reference's PNG frame of a padded conserved state Qh (host, g = 2):
+ * its extract_fields kernel, the ranges of its WRITE_FRAME (left panel 0 ..
+ * max(gpu_max, 1e-12), right panel the pressure's min .. max) and its
+ * write_png_2panel (keep_fv_euler_2d.cu:541-589, :671-681), into file `fn` */
+int refg_keep_frame(const double *Qh, int N, int lmv, const char *fn)
+{
+    const int Np = N + 2 * G_GHOST;
+    size_t nP = (size_t)4 * Np * Np, n1 = (size_t)N * N;
+    double *dQ = nullptr, *dl = nullptr, *dr = nullptr, *dt = nullptr;
+    RET_ON_ERR(cudaMalloc(&dQ, nP * sizeof(double)));
+    RET_ON_ERR(cudaMalloc(&dl, n1 * sizeof(double)));
+    RET_ON_ERR(cudaMalloc(&dr, n1 * sizeof(double)));
+    RET_ON_ERR(cudaMalloc(&dt, GS_NBLK * sizeof(double)));
+    RET_ON_ERR(cudaMemcpy(dQ, Qh, nP * sizeof(double), cudaMemcpyHostToDevice));
+    extract_fields<<<GS_NBLK, BLOCK1D>>>(dQ, dl, dr, N, Np, lmv);
+    RET_ON_ERR(cudaDeviceSynchronize());
+    double Lhi = gpu_max(dl, dt, N * N);
+    double *hl = (double *)malloc(n1 * sizeof(double)), *hr = (double *)malloc(n1 * sizeof(double));
+    RET_ON_ERR(cudaMemcpy(hl, dl, n1 * sizeof(double), cudaMemcpyDeviceToHost));
+    RET_ON_ERR(cudaMemcpy(hr, dr, n1 * sizeof(double), cudaMemcpyDeviceToHost));
+    double Rlo = 1e30, Rhi = -1e30;
+    for (size_t q = 0; q < n1; q++) { Rlo = fmin(Rlo, hr[q]); Rhi = fmax(Rhi, hr[q]); }
+    write_png_2panel(fn, hl, 0., fmax(Lhi, 1e-12), hr, Rlo, Rhi, N);
+    free(hl); free(hr);
+    cudaFree(dQ); cudaFree(dl); cudaFree(dr); cudaFree(dt);
+    return 0;
+}
+
+
 /* compute_ed + gpu_max + compute_rhs (keep_fv_euler_2d.cu:640-645) on host arrays */
 int refg_keep_rhs(const R *Qh, R *RHSh, R *lamh, int N, int Np, R h, R *edmax_out)
 {
