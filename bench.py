@@ -282,6 +282,7 @@ def e2e_run(F, torch, stream, precision, n, steps, dist):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s.set_state(host_in.numpy(), interior=True)
+    ta = time.perf_counter()
     for k in range(steps):
         s.step(1)
         s.post_stats(k % 2)
@@ -290,8 +291,10 @@ def e2e_run(F, torch, stream, precision, n, steps, dist):
             if st.status:
                 raise RuntimeError("step %d stopped with status %d" % (k, st.status))
     s.wait_stats((steps - 1) % 2)
+    tb = time.perf_counter()
     s.get_state(interior=True, out=host_out.numpy())
     t1 = time.perf_counter()
+    breakdown = {"upload_ms": (ta - t0) * 1e3, "steps_ms": (tb - ta) * 1e3, "download_ms": (t1 - tb) * 1e3}
     sec = R.max_over_ranks(t1 - t0, dist)
     # the two state transfers alone (upload with its layout conversion,
     # download with its conversion), best of three: with the device time of
@@ -309,7 +312,7 @@ def e2e_run(F, torch, stream, precision, n, steps, dist):
         down.append(c - b)
     s.close()
     state_bytes = 4 * n * n * 8
-    return sec, state_bytes / steps + 8, state_bytes / steps + 80, min(up), min(down), state_bytes
+    return sec, state_bytes / steps + 8, state_bytes / steps + 80, min(up), min(down), state_bytes, breakdown
 
 
 def small_forms(F, torch, plain_value):
@@ -404,10 +407,11 @@ def run_gpu(args):
             line["forms"].update(small_forms(F, torch, value))
 
     if not args.no_e2e:
-        sec, bi, bo, up_s, down_s, sbytes = e2e_run(F, torch, stream, args.precision, n, K, dist)
+        sec, bi, bo, up_s, down_s, sbytes, brk = e2e_run(F, torch, stream, args.precision, n, K, dist)
         line["e2e"] = {"value": world * units / sec, "unit": "cell-stage updates/s",
                        "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                        "state_upload_ms": up_s * 1e3, "state_download_ms": down_s * 1e3,
+                       "timed_region_ms": brk,
                        "link_gbs": {"h2d": sbytes / up_s / 1e9, "d2h": sbytes / down_s / 1e9},
                        # the steps' device time plus the two transfers, unoverlapped:
                        # the state must be whole on the device before the first dt
