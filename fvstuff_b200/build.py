@@ -29,7 +29,12 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
 # per-file flags: the rec3 and D2-viscosity kernels reproduce the
 # reference's arithmetic operation for operation, so no multiply-add
 # contraction there
-FILE_FLAGS = {"fvb_rec3.cu": ["-fmad=false"], "fvb_d2av.cu": ["-fmad=false"]}
+FILE_FLAGS = {"fvb_rec3.cu": ["-fmad=false"], "fvb_d2av.cu": ["-fmad=false"],
+              # the FP32-compensated kernel: single-precision denormals flushed
+              # to zero, so its reciprocals and square roots are the bare
+              # hardware approximations without the denormal-range fix-ups
+              # (its states, fluxes and increments are normal numbers)
+              "fvb_stage32c.cu": ["-ftz=true"]}
 
 
 def _run(cmd):

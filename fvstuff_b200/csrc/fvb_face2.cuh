@@ -89,8 +89,6 @@ __device__ __forceinline__ void face_flux(const V L[4], const V Rv[4], const V W
         const V rR = Rv[0], uR = Rv[1], tR = Rv[2], pR = Rv[3];
         const V cL = vsqrt(vmax(mul(mul(G, pL), rcp(rL)), tiny));
         const V cR = vsqrt(vmax(mul(mul(G, pR), rcp(rR)), tiny));
-        const V EL = fma(mul(half, rL), fma(uL, uL, mul(tL, tL)), mul(pL, IG));
-        const V ER = fma(mul(half, rR), fma(uR, uR, mul(tR, tR)), mul(pR, IG));
         const V SL = vmin(sub(uL, cL), sub(uR, cR)), SR = vmax(add(uL, cL), add(uR, cR));
         const V dL = mul(rL, sub(SL, uL)), dR = mul(rR, sub(SR, uR));
         const V Ss = mul(sub(fma(dL, uL, sub(pR, pL)), mul(dR, uR)), rcp(sub(dL, dR)));
@@ -99,8 +97,10 @@ __device__ __forceinline__ void face_flux(const V L[4], const V Rv[4], const V W
         const B sup{supL.x || SR.x <= 0.0f, supL.y || SR.y <= 0.0f};
         const B left{sup.x ? supL.x : Ss.x >= 0.0f, sup.y ? supL.y : Ss.y >= 0.0f};
         const V rK = sel(left, rL, rR), uK = sel(left, uL, uR), tK = sel(left, tL, tR);
-        const V pK = sel(left, pL, pR), EK = sel(left, EL, ER), SK = sel(left, SL, SR);
+        const V pK = sel(left, pL, pR), SK = sel(left, SL, SR);
         const V dK = sel(left, dL, dR);
+        // only side K's energy enters the flux: one evaluation, after the selection
+        const V EK = fma(mul(half, rK), fma(uK, uK, mul(tK, tK)), mul(pK, IG));
         // star weight: SK when subsonic, 0 when supersonic (q forced finite)
         const V SKw = sel(sup, zero, SK);
         const V q = sel(sup, zero, rcp(sub(SK, Ss)));

@@ -107,11 +107,6 @@ cudaError_t put_tile_maps(const CUtensorMap maps[TM_COUNT], CUtensorMap *dst, cu
 void *stage32c_fn(int shape, bool batched);
 size_t stage32c_smem(int shape);
 
-// the FP64 stage kernel laid out for three CTAs per SM (fvb_stage64.cu):
-// null where it is not instantiated (order, solver)
-void *stage64_fn(int order, int shape, int rs, bool batched);
-size_t stage64_smem(int order, int shape);
-
 // launchers (fvb_stage.cu).  rs: the solver on the reconstructed states of
 // the FP64 UP7 kernel -- 0 HLLC, 1 HLL, 2 Roe
 cudaError_t launch_stage(int prec, int order, int shape, const StageArgs &a, int grid_ctas,

@@ -31,12 +31,13 @@ template <class R> __device__ __forceinline__ R dabs(R a);
 template <> __device__ __forceinline__ float dabs<float>(float a) { return fabsf(a); }
 template <> __device__ __forceinline__ double dabs<double>(double a) { return fabs(a); }
 
-// floor used on reconstructed and updated rho and p (x > c ? x : c, so a
-// NaN becomes the floor, as in fv_up7_ducros_2d.cu:421-422, :543-544)
+// floor used on reconstructed and updated rho and p: x > c ? x : c, so a
+// NaN becomes the floor (fv_up7_ducros_2d.cu:421-422, :543-544).  fmax
+// gives that same value for every input (NaN, signed zeros and infinities
+// included) in one min/max instruction instead of a compare and two selects.
 template <class R> __device__ __forceinline__ R floor14(R x)
 {
-    const R c = FVB_LIT(R, 1e-14);
-    return x > c ? x : c;
+    return dmax<R>(x, FVB_LIT(R, 1e-14));
 }
 
 // Gas constants of one solver.  gm1 is formed as gamma - 1 at run time, the
@@ -406,8 +407,6 @@ __device__ __forceinline__ void recon_flux_fast(const R L[4], const R Rv[4], con
             cL = fsqrt(cs2L > FVB_LIT(R, 1e-14) ? cs2L : FVB_LIT(R, 1e-14));
             cR = fsqrt(cs2R > FVB_LIT(R, 1e-14) ? cs2R : FVB_LIT(R, 1e-14));
         }
-        const R EL = pL * gs.igm1 + R(0.5) * rL * (uL * uL + tL * tL);
-        const R ER = pR * gs.igm1 + R(0.5) * rR * (uR * uR + tR * tR);
         const R SL = dmin<R>(uL - cL, uR - cR), SR = dmax<R>(uL + cL, uR + cR);
         const R dL = rL * (SL - uL), dR = rR * (SR - uR);
         const R Ss = (pR - pL + dL * uL - dR * uR) * frcp(dL - dR);
@@ -416,8 +415,11 @@ __device__ __forceinline__ void recon_flux_fast(const R L[4], const R Rv[4], con
         const bool sup = supL || (SR <= zero);
         const bool left = sup ? supL : (Ss >= zero);
         const R rK = left ? rL : rR, uK = left ? uL : uR, tK = left ? tL : tR;
-        const R pK = left ? pL : pR, EK = left ? EL : ER, SK = left ? SL : SR;
+        const R pK = left ? pL : pR, SK = left ? SL : SR;
         const R dK = left ? dL : dR;
+        // only side K's energy enters the flux: one evaluation, after the
+        // selection (the same expression as for either side)
+        const R EK = pK * gs.igm1 + R(0.5) * rK * (uK * uK + tK * tK);
         // star terms weighted by SK, or by 0 when supersonic (q forced
         // finite), so one set of expressions gives both fluxes.  With
         // dK = rK (SK - uK) and q = 1 / (SK - Ss):  fact = dK q, and

@@ -21,7 +21,6 @@
 #include <stdint.h>
 
 #include <algorithm>
-#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -433,21 +432,9 @@ static KernelEntry entry32c(int shape)
     entry<P64, 7, 0, RS>(), entry<P64, 7, 1, RS>(), entry<P64, 7, 2, RS>(), entry<P64, 7, 3, RS>(), \
         entry<P64, 7, 4, RS>(), entry<P64, 7, 5, RS>()
 
-static KernelEntry entry64(int order, int shape, int rs)
-{
-    return KernelEntry{stage64_fn(order, shape, rs, false), stage64_fn(order, shape, rs, true),
-                       stage64_smem(order, shape), kTileShapes[shape].nt};
-}
-
 static KernelEntry *table_for(int prec, int order, int rs = 0)
 {
-    static const bool lean = [] {
-        const char *e = std::getenv("FVB_K64");
-        return !(e && e[0] == '1');
-    }();
-    static KernelEntry t64l_7[] = {entry64(7, 0, 0), entry64(7, 1, 0), entry64(7, 2, 0),
-                                   entry64(7, 3, 0), entry64(7, 4, 0), entry64(7, 5, 0)};
-    if (lean && prec == P64 && order == 7 && rs == 0) return t64l_7;
+
     static KernelEntry t64_7_hll[] = {FVB_SHAPES_RS(1)};
     static KernelEntry t64_7_roe[] = {FVB_SHAPES_RS(2)};
     if (rs != 0) return (prec == P64 && order == 7) ? (rs == 1 ? t64_7_hll : rs == 2 ? t64_7_roe : nullptr) : nullptr;

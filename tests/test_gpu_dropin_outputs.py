@@ -94,8 +94,9 @@ def _masked(text):
 
 
 def _shape(line):
-    """a line with every number replaced by '#'"""
-    return _NUM.sub("#", line)
+    """a line with every number replaced by '#' and runs of blanks by one
+    (printf field widths pad numbers of different lengths differently)"""
+    return re.sub(r"\s+", " ", _NUM.sub("#", line))
 
 
 def _run(cmd, cwd):
