@@ -88,14 +88,13 @@ struct StageArgs {
 
 // Tile shapes the stage kernel is instantiated for (tile width x height,
 // threads per CTA).  Chosen so the face count (TX+1)TY + TX(TY+1) is close
-// to a multiple of the thread count.  The square shape gives the
-// FP32-compensated form its transposed-pair kernel (fvb_stage32c.cu).
+// to a multiple of the thread count.
 struct TileShape {
     int tx, ty, nt;
 };
-constexpr int kNumTileShapes = 7;
+constexpr int kNumTileShapes = 6;
 constexpr TileShape kTileShapes[kNumTileShapes] = {
-    {32, 15, 256}, {32, 7, 128}, {64, 7, 256}, {16, 15, 256}, {32, 9, 256}, {32, 16, 256}, {20, 20, 224}};
+    {32, 15, 256}, {32, 7, 128}, {64, 7, 256}, {16, 15, 256}, {32, 9, 256}, {32, 16, 256}};
 
 // TMA descriptors (fvb_stage.cu): encode the four maps of a grid for a
 // tile shape into host memory; false if this grid cannot use TMA

@@ -328,315 +328,12 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
     if (s_err && gd_has_tma(a)) mbar_wait(&s_bar, phase);
 }
 
-// ---------------------------------------------------------------------------
-// Square-tile variant.  With a T x T tile, x-face (r, c) -- between cells
-// (r, c-1) and (r, c) -- and y-face (c, r) -- between cells (c-1, r) and
-// (c, r) -- are each other's transpose, and every one of the T (T+1) x-faces
-// has exactly one such partner.  The working box is kept as interleaved
-// pairs W2[m][r][c] = (x-frame value of cell (r, c), y-frame value of cell
-// (c, r)), variables m = rho, normal velocity, tangential velocity, p, so the
-// two stencils of a face pair lie at the same (row, column) of W2: one 64-bit
-// shared-memory load gives a stencil point for both faces (32 loads a pair
-// instead of 64), and likewise the sound speed and energy (CE2) and the
-// stored fluxes (FXY[q][r][c] = (x-face flux, y-face flux), Cartesian q).
-// The conversion takes cell (r, c) and cell (c, r) of the box together, so
-// its arithmetic is packed too.  Results are the same expressions as the
-// kernel above, face for face.
-// ---------------------------------------------------------------------------
-template <int T, int NT, bool BATCHED>
-__global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32t_kernel(const __grid_constant__ StageArgs a)
-{
-    constexpr int G = 4;
-    constexpr int S = T + 2 * G, PL = S * S;   // box side and plane
-    constexpr int CS = T + 2, CPL = CS * CS;   // the cells the HLLE reads: box rows / columns [G-1, G+T]
-    constexpr int NP = T * (T + 1);            // face pairs
-    constexpr int NC = T * T;
-    constexpr int NPAIR = S * (S + 1) / 2;     // box cells (r, c), r <= c, with their transposes
-    constexpr int NW = NT / 32;
-    static_assert(S <= 255, "pair table holds bytes");
-
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float *IN = reinterpret_cast<float *>(smem_raw);           // [8][S][S]: hi (+ increment) as loaded
-    float2 *W2 = reinterpret_cast<float2 *>(IN + 8 * PL);      // [4][S][S]
-    float2 *CE2 = W2 + 4 * PL;                                  // [2][CS][CS]: c, E
-    float2 *FXY = CE2 + 2 * CPL;                                // [4][T][T+1]
-    unsigned short *PAIRS = reinterpret_cast<unsigned short *>(FXY + 4 * T * (T + 1));  // [NPAIR]: r << 8 | c
-    __shared__ double s_red[NW];
-    __shared__ __align__(8) uint64_t s_bar;
-    __shared__ int s_err;
-    __shared__ __align__(16) TileHdr s_hdr[2];
-    __shared__ TileRef s_ref_next;
-
-    const int tid = threadIdx.x;
-    constexpr bool batched = BATCHED;
-    const int ntiles = batched ? *a.ntiles : a.ntiles_static;
-    const int cur = a.parity, nxt = a.parity ^ 1;
-    if (tid == 0) {
-        mbar_init(&s_bar, 1);
-        s_err = 0;
-    }
-    // the upper triangle of the box, row by row: pair k -> (r, c), c >= r
-    for (int k = tid; k < NPAIR; k += NT) {
-        int r = 0, start = 0;
-        while (start + (S - r) <= k) { start += S - r; ++r; }
-        PAIRS[k] = (unsigned short)((r << 8) | (r + (k - start)));
-    }
-    __syncthreads();
-
-    uint32_t phase = 0;
-    auto wait_box = [&](bool tma) {
-        if (tma) {
-            if (mbar_wait(&s_bar, phase)) phase ^= 1;
-            else s_err = 1;
-        }
-        __syncthreads();
-    };
-    auto start_single = [&](int t) -> bool {
-        if (tid == 0 && a.grid.tmap) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue_tile_load<P32C, G, S, S, NT>(a.grid, a.stage, cur, t, IN, &s_bar, tid);
-        return a.grid.tmap != nullptr;
-    };
-    const bool drop = !batched && blockIdx.x == 0 && a.stage > 0 && a.grid.ctrl && a.grid.tmap &&
-                      *(volatile int *)&a.grid.ctrl->drop_load;
-    const int stride = gridDim.x;
-    int t = blockIdx.x, slot = 0;
-    if (t < ntiles && batched) {
-        if (tid < 32) {
-            const TileRef r0 = a.tiles[t];
-            start_batched_tile<P32C, G, S, S, NT>(a, &s_hdr[0], r0, hdr_word(a, r0, tid), cur, IN, &s_bar, tid);
-            if (tid == 0 && t + stride < ntiles) s_ref_next = a.tiles[t + stride];
-        }
-        wait_box(true);
-    } else if (drop) {
-        wait_box(true);  // nothing was issued: the wait runs out
-        if (tid == 0) a.grid.ctrl->drop_load = 0;
-    } else {
-        wait_box(t < ntiles ? start_single(t) : false);
-    }
-    double lacc = 0.0;
-    TileCtl ctl1{};
-    if (!batched && t < ntiles) ctl1 = tile_control<P32C>(a.grid.ctrl, a.stage, tid == 0 && t == 0);
-    for (; t < ntiles; t += stride, slot ^= 1) {
-        const bool has_next = t + stride < ntiles;
-        unsigned long long wnext = 0ull;
-        TileRef ref_next{}, ref_after{};
-        if (batched && tid < 32) {
-            if (has_next) {
-                ref_next = s_ref_next;
-                wnext = hdr_word(a, ref_next, tid);
-            }
-            if (t + 2 * stride < ntiles) ref_after = a.tiles[t + 2 * stride];
-        }
-        const GridDev &gd = tile_grid<BATCHED>(s_hdr[slot], a);
-        const int tile = batched ? s_hdr[slot].tile : t;
-        const TileCtl ctl = batched ? s_hdr[slot].ctl : ctl1;
-        const int n = gd.n;
-        const int tx0 = (tile % gd.tiles_x) * T, ty0 = (tile / gd.tiles_x) * T;
-        const float gam = (float)gd.gam, gm1 = (float)gd.gam - 1.0f, igm1 = (float)(1.0 / (gd.gam - 1.0));
-        if (s_err) {
-            if (tid == 0 && gd.ctrl) gd.ctrl->status = FVB_ERR_TIMEOUT;
-            break;
-        }
-        // ---- 1. stage input U0 + d of box cells (r, c) and (c, r) together:
-        //         primitives into W2, sound speed and energy into CE2 --------
-        if (ctl.run) {
-            const f2::V G2 = f2::splat(gam), GM1 = f2::splat(gm1), HALF = f2::splat(0.5f);
-            for (int k = tid; k < NPAIR; k += NT) {
-                const int rc = PAIRS[k], r = rc >> 8, c = rc & 255;
-                const int ka = r * S + c, kb = c * S + r;
-                f2::V w[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) w[q] = make_float2(IN[q * PL + ka], IN[q * PL + kb]);
-                if (a.stage >= 2) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        w[q] = f2::add(w[q], make_float2(IN[(4 + q) * PL + ka], IN[(4 + q) * PL + kb]));
-                }
-                const f2::V ir = f2::rcp(w[0]);
-                const f2::V E = w[3];
-                w[1] = f2::mul(w[1], ir);
-                w[2] = f2::mul(w[2], ir);
-                // p = (gamma - 1) (E - rho (u^2 + v^2) / 2)
-                w[3] = f2::mul(GM1, f2::fms(f2::mul(HALF, w[0]), f2::fma(w[1], w[1], f2::mul(w[2], w[2])), E));
-                w[3] = make_float2(-w[3].x, -w[3].y);
-                // x lane of (r, c) is cell A = (r, c); y lane of (r, c) is cell B = (c, r) in its y frame
-                W2[ka] = w[0];
-                W2[PL + ka] = make_float2(w[1].x, w[2].y);
-                W2[2 * PL + ka] = make_float2(w[2].x, w[1].y);
-                W2[3 * PL + ka] = w[3];
-                if (kb != ka) {
-                    W2[kb] = make_float2(w[0].y, w[0].x);
-                    W2[PL + kb] = make_float2(w[1].y, w[2].x);
-                    W2[2 * PL + kb] = make_float2(w[2].y, w[1].x);
-                    W2[3 * PL + kb] = make_float2(w[3].y, w[3].x);
-                }
-                const int rr = r - (G - 1), cc = c - (G - 1);
-                if ((unsigned)rr < (unsigned)CS && (unsigned)cc < (unsigned)CS) {
-                    const f2::V cs2 = f2::vmax(f2::mul(f2::mul(G2, w[3]), ir), f2::splat(1e-14f));
-                    const f2::V cv = f2::vsqrt(cs2);
-                    const int ca = rr * CS + cc, cb = cc * CS + rr;
-                    CE2[ca] = cv;
-                    CE2[CPL + ca] = E;
-                    if (cb != ca) {
-                        CE2[cb] = make_float2(cv.y, cv.x);
-                        CE2[CPL + cb] = make_float2(E.y, E.x);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        // ---- 2. load the next tile into IN (asynchronous through TMA) -------
-        bool next_tma = false;
-        if (has_next) {
-            if (batched) {
-                if (tid < 32) {
-                    start_batched_tile<P32C, G, S, S, NT>(a, &s_hdr[slot ^ 1], ref_next, wnext, cur, IN, &s_bar, tid);
-                    if (tid == 0) s_ref_next = ref_after;
-                }
-                next_tma = true;
-            } else {
-                next_tma = start_single(t + stride);
-            }
-        }
-        if (!ctl.run) {
-            if (ctl.copy) {
-                // skipped step: the next step reads the other buffer
-                const float *hi = (const float *)gd.st[cur], *lo = (const float *)gd.lo[cur];
-                for (int k = tid; k < NC; k += NT) {
-                    int r = k / T, c = k - r * T, i = tx0 + c, j = ty0 + r;
-                    if (i >= n || j >= n) continue;
-                    float vh[4], vl[4];
-                    long long e = gidx(gd, 0, j, i);
-                    for (int q = 0; q < 4; ++q) { vh[q] = hi[e + q * gd.plane]; vl[q] = lo[e + q * gd.plane]; }
-                    put_cell2<float>(gd, (float *)gd.st[nxt], (float *)gd.lo[nxt], j, i, vh, vl);
-                }
-            }
-            wait_box(next_tma);
-            continue;
-        }
-        const float dt = (float)ctl.dt;
-        const float dt_h = dt * (float)(1.0 / gd.h);
-
-        // ---- 3. face pairs: x-face (r, c) with y-face (c, r) ----------------
-        for (int p = tid; p < NP; p += NT) {
-            const int r = p / (T + 1), c = p - r * (T + 1);
-            const float2 *base = W2 + (r + G) * S + c;   // stencil points d = 0..7 at base[d]
-            f2::V L[4], Rv[4], WL[4], WR[4];
-#pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                f2::V sv[8];
-#pragma unroll
-                for (int d = 0; d < 8; ++d) sv[d] = base[m * PL + d];
-                f2::upface7(sv, L[m], Rv[m]);
-                WL[m] = sv[G - 1];
-                WR[m] = sv[G];
-            }
-            const f2::V tiny = f2::splat(1e-14f);
-            L[0] = f2::vmax(L[0], tiny); Rv[0] = f2::vmax(Rv[0], tiny);
-            L[3] = f2::vmax(L[3], tiny); Rv[3] = f2::vmax(Rv[3], tiny);
-            const float2 *ce = CE2 + (r + 1) * CS + c;
-            f2::V F[4];
-            f2::face_flux(L, Rv, WL, WR, ce[0], ce[1], ce[CPL], ce[CPL + 1], gam, igm1, F);
-            float2 *o = FXY + r * (T + 1) + c;
-            constexpr int os = T * (T + 1);
-            // Cartesian components: the y lane's normal momentum is v, its tangential u
-            o[0] = F[0];
-            o[os] = make_float2(F[1].x, F[2].y);
-            o[2 * os] = make_float2(F[2].x, F[1].y);
-            o[3 * os] = F[3];
-        }
-        __syncthreads();
-
-        // ---- 4. divergence, RK combination, stores --------------------------
-        float lmax = 0.0f;
-        for (int k = tid; k < NC; k += NT) {
-            const int r = k / T, c = k - r * T, i = tx0 + c, j = ty0 + r;
-            if (i >= n || j >= n) continue;
-            float dres[4];  // dt L
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float2 *f = FXY + q * T * (T + 1);
-                // x faces of cell (r, c): pairs (r, c), (r, c+1); y faces: pairs (c, r), (c, r+1)
-                const float fxl = f[r * (T + 1) + c].x, fxr = f[r * (T + 1) + c + 1].x;
-                const float fyb = f[c * (T + 1) + r].y, fyt = f[c * (T + 1) + r + 1].y;
-                dres[q] = -((fxr - fxl) + (fyt - fyb)) * dt_h;
-            }
-            if (a.stage == 1) {
-                put_cell<float>(gd, (float *)gd.k1, j, i, dres);
-            } else if (a.stage == 2) {
-                float d[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float d1 = ((const float *)gd.k1)[gidx(gd, q, j, i)];
-                    d[q] = 0.25f * (d1 + dres[q]);
-                }
-                put_cell<float>(gd, (float *)gd.k2, j, i, d);
-            } else {
-                float vh[4], vl[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const long long e = gidx(gd, q, j, i);
-                    const float d = (2.0f / 3.0f) * (((const float *)gd.k2)[e] + dres[q]);
-                    vh[q] = ((const float *)gd.st[cur])[e];
-                    vl[q] = ((const float *)gd.lo[cur])[e];
-                    df_add(vh[q], vl[q], d);
-                }
-                float w[4];
-                {
-                    const float ir = frcp(vh[0]);
-                    w[0] = vh[0]; w[1] = vh[1] * ir; w[2] = vh[2] * ir;
-                    w[3] = gm1 * (vh[3] - 0.5f * (vh[1] * vh[1] + vh[2] * vh[2]) * ir);
-                }
-                if (!(w[0] > 1e-14f)) { vh[0] = 1e-14f; vl[0] = 0.f; w[0] = 1e-14f; }
-                if (!(w[3] > 1e-14f)) {
-                    float ke = 0.5f * (vh[1] * vh[1] + vh[2] * vh[2]) / vh[0];
-                    vh[3] = 1e-14f / gm1 + ke; vl[3] = 0.f; w[3] = 1e-14f;
-                }
-                put_cell2<float>(gd, (float *)gd.st[nxt], (float *)gd.lo[nxt], j, i, vh, vl);
-                float cs2 = gam * w[3] * frcp(w[0]);
-                float lam = fabsf(w[1]) + fabsf(w[2]) + fsqrt(cs2 > 1e-14f ? cs2 : 1e-14f);
-                lmax = fmaxf(lmax, lam);
-            }
-        }
-
-        // ---- 5. max wave speed of the new state (stage 3) ------------------
-        if (a.stage == 3) {
-            if (!batched && tid == 0 && tile == 0) leader_finish<P32C>(gd.ctrl);
-            if (batched) {
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-                if ((tid & 31) == 0 && lmax > 0.0f)
-                    atomicMax(&gd.ctrl->lam_acc, (unsigned long long)__double_as_longlong((double)lmax));
-            } else {
-                lacc = fmax(lacc, (double)lmax);
-            }
-        }
-        wait_box(next_tma);
-    }
-    if (!batched && a.stage == 3) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) lacc = fmax(lacc, __shfl_xor_sync(0xffffffffu, lacc, o));
-        if ((tid & 31) == 0) s_red[tid >> 5] = lacc;
-        __syncthreads();
-        if (tid == 0 && a.grid.ctrl) {
-            double m = 0.0;
-            for (int w = 0; w < NW; ++w) m = fmax(m, s_red[w]);
-            if (m > 0.0) atomicMax(&a.grid.ctrl->lam_acc, (unsigned long long)__double_as_longlong(m));
-        }
-    }
-    if (s_err && gd_has_tma(a)) mbar_wait(&s_bar, phase);
-}
-
 template <int SHAPE>
 static void *fn32c(bool batched)
 {
     constexpr TileShape ts = kTileShapes[SHAPE];
-    // square tiles take the transposed-pair kernel
-    if constexpr (ts.tx == ts.ty)
-        return batched ? (void *)stage32t_kernel<ts.tx, ts.nt, true> : (void *)stage32t_kernel<ts.tx, ts.nt, false>;
-    else
-        return batched ? (void *)stage32c_kernel<ts.tx, ts.ty, ts.nt, true>
-                       : (void *)stage32c_kernel<ts.tx, ts.ty, ts.nt, false>;
+    return batched ? (void *)stage32c_kernel<ts.tx, ts.ty, ts.nt, true>
+                   : (void *)stage32c_kernel<ts.tx, ts.ty, ts.nt, false>;
 }
 
 void *stage32c_fn(int shape, bool batched)
@@ -648,7 +345,6 @@ void *stage32c_fn(int shape, bool batched)
     case 3: return fn32c<3>(batched);
     case 4: return fn32c<4>(batched);
     case 5: return fn32c<5>(batched);
-    case 6: return fn32c<6>(batched);
     default: return nullptr;
     }
 }
@@ -658,12 +354,6 @@ size_t stage32c_smem(int shape)
     if (shape < 0 || shape >= kNumTileShapes) return 0;
     const TileShape &ts = kTileShapes[shape];
     const int sw = ts.tx + 8, sh = ts.ty + 8;
-    if (ts.tx == ts.ty) {
-        // IN (8 planes of floats), W2 (4 planes of pairs), CE2, FXY, pair table
-        const size_t pl = (size_t)sw * sw, cpl = (size_t)(ts.tx + 2) * (ts.tx + 2);
-        return sizeof(float) * 8 * pl + sizeof(float2) * (4 * pl + 2 * cpl + 4 * (size_t)ts.tx * (ts.tx + 1)) +
-               sizeof(unsigned short) * (size_t)sw * (sw + 1) / 2;
-    }
     return sizeof(float) * ((size_t)14 * sw * sh + 4 * ts.ty * (ts.tx + 1) + 4 * (ts.ty + 1) * ts.tx);
 }
 
