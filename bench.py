@@ -50,10 +50,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--mode", default="plain",
-                   choices=["plain", "batched", "serve", "large", "families", "precision"],
+                   choices=["plain", "batched", "serve", "large", "families", "precision", "aux"],
                    help="plain: the headline line; batched / serve / large: the other configurations; "
                         "families: the other flux families on their own cases; precision: FP32c against "
-                        "FP64 over a whole run")
+                        "FP64 over a whole run; aux: the auxiliary kernels' bandwidth")
     p.add_argument("--t-end", type=float, default=1.0, help="precision: final time of the KH run")
     p.add_argument("--families", default="up_ducros_hll,up_ducros_roe,keep,rec3,up_hllc_d2av",
                    help="families: which ones")
@@ -79,7 +79,7 @@ def parse():
     if a.n is None:
         a.n = 8192 if large else 2048
     if a.steps is None:
-        a.steps = 2000 if large else 50 if a.mode == "families" else 400
+        a.steps = 2000 if large else 50 if a.mode == "families" else 20 if a.mode == "aux" else 400
     return a
 
 
@@ -885,6 +885,72 @@ def run_precision(args):
     print(json.dumps(line), flush=True)
 
 
+def run_aux(args):
+    """The library's kernels other than the stage kernels, FP64 at n^2 on
+    one GPU: each entry point timed with CUDA events on its stream (median of
+    --steps repetitions after --warmup), against the bytes it must move."""
+    import torch
+
+    import fvstuff_b200 as F
+    n, K, W = args.n, max(1, args.steps), max(1, args.warmup)
+    np_ = n + 8
+    st = torch.cuda.current_stream()
+    h = st.cuda_stream
+    s = F.Solver(n, bc="periodic", cfl=0.5, precision="f64", stream=h)
+    s.init_case("kh")
+    dev = dict(dtype=torch.float64, device="cuda")
+    Q = torch.empty((4, np_, np_), **dev)
+    s.get_state(out=Q)
+    U0, Uk, Uo = Q.clone(), Q.clone(), torch.empty_like(Q)
+    rhs, lam, mx = torch.zeros((4, n, n), **dev), torch.zeros((n, n), **dev), torch.zeros(1, **dev)
+    state, cells, ghost = 4 * np_ * np_ * 8, 4 * n * n * 8, 4 * (np_ * np_ - n * n) * 8
+    items = [
+        ("fvb_set_state (device IDX_P in: import, ghost ring, wave-speed max, step control)",
+         lambda: s.set_state(Q), state + state + cells),
+        ("fvb_get_state (device IDX_P out: export)", lambda: s.get_state(out=Q), state + state),
+        ("fvb_apply_bc (ghost ring of a caller array, periodic)", lambda: F.apply_bc(Q, n, np_, "periodic"), 2 * ghost),
+        ("fvb_up_rhs (residual and wave speeds of a caller array)",
+         lambda: F.up_rhs(Q, rhs, lam, n, np_, 1.0 / n, stream=h), state + cells + n * n * 8),
+        ("fvb_rk3_stage (stage 2 on caller arrays)",
+         lambda: F.rk3_stage(2, Uo, U0, Uk, rhs, 1e-4, n, np_, stream=h), 3 * cells + cells),
+        ("fvb_max (n^2 doubles)", lambda: F.device_max(lam, mx, stream=h), n * n * 8),
+        ("fvb_stats_sums (conserved FP64 sums of the state)", lambda: s.stats(), cells),
+        # (the device part on the solver's stream; the copy to the host runs
+        # on a second stream and is collected outside the timed region)
+        ("fvb_frame_begin (device part: FP32 export, frame fields)", s.frame_begin,
+         cells + cells // 2 + cells // 2 + 5 * n * n * 4, s.frame_end),
+    ]
+    hbm, peak_kind = peaks()
+    out = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        for name, fn, nbytes, *post in items:
+            after = post[0] if post else (lambda: None)
+            for _ in range(W):
+                fn()
+                after()
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(K):
+                e0.record(st)
+                fn()
+                e1.record(st)
+                e1.synchronize()
+                after()
+                ts.append(e0.elapsed_time(e1))
+            ms = statistics.median(ts)
+            out.append({"entry": name, "ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6,
+                        "roofline_frac": nbytes / ms / 1e6 / hbm})
+            print("%-80s %8.3f ms %8.1f GB/s" % (name, ms, nbytes / ms / 1e6), file=sys.stderr, flush=True)
+    s.close()
+    line = {"metric": METRIC, "value": None, "unit": "GB/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic", "mode": "aux",
+            "config": {"workload": "the library's auxiliary kernels on a %dx%d FP64 state (KH), caller arrays in "
+                                   "the reference's IDX_P layout; larger than L2" % (n, n)},
+            "peak_gbs": hbm, "peak_kind": peak_kind, "kernels": out, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -899,6 +965,8 @@ def main():
         run_families(args)
     elif args.mode == "precision":
         run_precision(args)
+    elif args.mode == "aux":
+        run_aux(args)
     else:
         run_gpu(args)
 
