@@ -894,7 +894,10 @@ def run_aux(args):
     import fvstuff_b200 as F
     n, K, W = args.n, max(1, args.steps), max(1, args.warmup)
     np_ = n + 8
-    st = torch.cuda.current_stream()
+    # one stream for the solver, the caller arrays and the events: a
+    # library call on any other stream would leave the events around nothing
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
     h = st.cuda_stream
     s = F.Solver(n, bc="periodic", cfl=0.5, precision="f64", stream=h)
     s.init_case("kh")
@@ -908,7 +911,7 @@ def run_aux(args):
         ("fvb_set_state (device IDX_P in: import, ghost ring, wave-speed max, step control)",
          lambda: s.set_state(Q), state + state + cells),
         ("fvb_get_state (device IDX_P out: export)", lambda: s.get_state(out=Q), state + state),
-        ("fvb_apply_bc (ghost ring of a caller array, periodic)", lambda: F.apply_bc(Q, n, np_, "periodic"), 2 * ghost),
+        ("fvb_apply_bc (ghost ring of a caller array, periodic)", lambda: F.apply_bc(Q, n, np_, "periodic", stream=h), 2 * ghost),
         ("fvb_up_rhs (residual and wave speeds of a caller array)",
          lambda: F.up_rhs(Q, rhs, lam, n, np_, 1.0 / n, stream=h), state + cells + n * n * 8),
         ("fvb_rk3_stage (stage 2 on caller arrays)",

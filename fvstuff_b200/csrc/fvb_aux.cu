@@ -10,6 +10,20 @@
 
 namespace fvb {
 
+// row j and column i of cell k of an n x n grid (k = j n + i): a 32-bit
+// unsigned division while k fits, the 64-bit one only beyond
+__device__ __forceinline__ void cell_rc(long long k, int n, int &j, int &i)
+{
+    if (k <= 0xffffffffll) {
+        const unsigned u = (unsigned)k, jj = u / (unsigned)n;
+        j = (int)jj;
+        i = (int)(u - jj * (unsigned)n);
+    } else {
+        j = (int)(k / n);
+        i = (int)(k - (long long)j * n);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // ghost ring
 // ---------------------------------------------------------------------------
@@ -92,7 +106,8 @@ __global__ void ic_kernel(double *out, int n, double x0, double y0, double h, do
     const long long n2 = (long long)n * n;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
          k += (long long)blockDim.x * gridDim.x) {
-        const int j = (int)(k / n), i = (int)(k % n);
+        int j, i;
+        cell_rc(k, n, j, i);
         const double x = x0 + (i + 0.5) * h, y = y0 + (j + 0.5) * h;
         double r = 1, u = 0, v = 0, p = 1;
         switch (c.kind) {
@@ -193,7 +208,8 @@ __global__ void ic_sod32_kernel(float *out, int n, float x0, float y0, float h, 
     const long long n2 = (long long)n * n;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
          k += (long long)blockDim.x * gridDim.x) {
-        const int j = (int)(k / n), i = (int)(k % n);
+        int j, i;
+        cell_rc(k, n, j, i);
         const float xc = x0 + (i + 0.5f) * h, yc = y0 + (j + 0.5f) * h;
         const float r = sqrtf((xc - xc0) * (xc - xc0) + (yc - yc0) * (yc - yc0));
         const float delta = 1.0f * h;
@@ -261,7 +277,8 @@ __global__ void import_kernel(const void *src, ExtView e, void *dst, void *dst_l
     const long long n2 = (long long)n * n;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
          k += (long long)blockDim.x * gridDim.x) {
-        const int j = (int)(k / n), i = (int)(k % n);
+        int j, i;
+        cell_rc(k, n, j, i);
         long long es = e.interior ? k : (long long)(j + e.g) * e.np + (i + e.g);
         long long eplane = e.interior ? n2 : (long long)e.np * e.np;
         double x[4];
@@ -307,7 +324,8 @@ __global__ void export_kernel(const void *src, const void *src_lo, BufView v, in
     const int eo = e.interior ? 0 : e.g - v.g;     // caller's padded offset of the same cell
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cnt;
          k += (long long)blockDim.x * gridDim.x) {
-        const int jj = (int)(k / span), ii = (int)(k % span);
+        int jj, ii;
+        cell_rc(k, span, jj, ii);
         const int jp = jj + off, ip = ii + off;
         long long s = (long long)jp * v.pitch + ip + v.xoff;
         double x[4];
@@ -373,7 +391,8 @@ __global__ void lam_kernel(const void *st, BufView v, int internal, double gam, 
     double m = 0.0;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
          k += (long long)blockDim.x * gridDim.x) {
-        const int j = (int)(k / n), i = (int)(k % n);
+        int j, i;
+        cell_rc(k, n, j, i);
         long long s = (long long)(j + v.g) * v.pitch + (i + v.g) + v.xoff;
         double lam;
         if (internal == INT_PRIM64) {
@@ -418,7 +437,8 @@ __global__ void sums_kernel(const void *st, const void *lo, BufView v, int inter
     double acc[5] = {0, 0, 0, 0, 0};
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
          k += (long long)blockDim.x * gridDim.x) {
-        const int j = (int)(k / n), i = (int)(k % n);
+        int j, i;
+        cell_rc(k, n, j, i);
         long long s = (long long)(j + v.g) * v.pitch + (i + v.g) + v.xoff;
         double c[4];
         if (internal == INT_CONS64) {
@@ -467,7 +487,8 @@ __global__ void rk3_kernel(int stage, R *Uo, const R *U0, const R *Uk, const R *
     const long long n2 = (long long)n * n, np2 = (long long)np * np;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2;
          k += (long long)blockDim.x * gridDim.x) {
-        const int j = (int)(k / n), i = (int)(k % n);
+        int j, i;
+        cell_rc(k, n, j, i);
         const long long c = (long long)(j + g) * np + (i + g);
         R w0[4], c0[4], cv[4], w[4];
         for (int q = 0; q < 4; ++q) w0[q] = U0[q * np2 + c];
@@ -575,11 +596,14 @@ __device__ __forceinline__ float frame_ducros(float pa, float pb)
     return dp * dp / (dp * dp + 0.1f * ps * ps);
 }
 
-__global__ void frame_kernel(const float *Q, int n, int g, int np, float h, float *out)
+// One thread per cell, 32 x 8 cells a block: the x-neighbours of a warp are
+// one coalesced row, the y-neighbours rows a block shares through L1.
+__global__ void __launch_bounds__(256) frame_kernel(const float *Q, int n, int g, int np, float h, float *out)
 {
     const long long nn = (long long)n * n;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn; k += (long long)gridDim.x * blockDim.x) {
-        const int j = (int)(k / n), i = (int)(k - (long long)j * n);
+    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+    if (i < n && j < n) {
+        const long long k = (long long)j * n + i;
         const long long pl = (long long)np * np;
         auto at = [&](int q, int jp, int ip) { return Q[q * pl + (long long)jp * np + ip]; };
         const int jp = j + g, ip = i + g;
@@ -619,7 +643,7 @@ __global__ void frame_kernel(const float *Q, int n, int g, int np, float h, floa
 
 cudaError_t frame_fields(const float *prim, int n, int g, int np, double h, float *out, cudaStream_t s)
 {
-    frame_kernel<<<592, 256, 0, s>>>(prim, n, g, np, (float)h, out);
+    frame_kernel<<<dim3((n + 31) / 32, (n + 7) / 8), dim3(32, 8), 0, s>>>(prim, n, g, np, (float)h, out);
     return cudaGetLastError();
 }
 
