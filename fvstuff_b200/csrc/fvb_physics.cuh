@@ -31,13 +31,28 @@ template <class R> __device__ __forceinline__ R dabs(R a);
 template <> __device__ __forceinline__ float dabs<float>(float a) { return fabsf(a); }
 template <> __device__ __forceinline__ double dabs<double>(double a) { return fabs(a); }
 
+// Min / max as one compare and a select, for the FP64 throughput paths.  An
+// FP64 fmin / fmax is not one instruction on sm_100: with its NaN rules it
+// issues about 7.5 (a compare, selects, integer and bit operations; ncu
+// op-class counters of a loop of them), a compare and a select 3.  smax(a, b)
+// is a > b ? a : b, smin(a, b) is a < b ? a : b: for finite operands the
+// value fmax / fmin give (up to the sign of a zero result), and with a
+// constant second operand (the clamps at 0, 1e-10, 1e-14) for every first
+// operand, NaN included (NaN -> the constant).  FP32 keeps fminf / fmaxf,
+// one instruction.
+template <class R> __device__ __forceinline__ R smin(R a, R b);
+template <> __device__ __forceinline__ float smin<float>(float a, float b) { return fminf(a, b); }
+template <> __device__ __forceinline__ double smin<double>(double a, double b) { return a < b ? a : b; }
+template <class R> __device__ __forceinline__ R smax(R a, R b);
+template <> __device__ __forceinline__ float smax<float>(float a, float b) { return fmaxf(a, b); }
+template <> __device__ __forceinline__ double smax<double>(double a, double b) { return a > b ? a : b; }
+
 // floor used on reconstructed and updated rho and p: x > c ? x : c, so a
-// NaN becomes the floor (fv_up7_ducros_2d.cu:421-422, :543-544).  fmax
-// gives that same value for every input (NaN, signed zeros and infinities
-// included) in one min/max instruction instead of a compare and two selects.
+// NaN becomes the floor (fv_up7_ducros_2d.cu:421-422, :543-544); the same
+// value as fmax(x, c) for every input
 template <class R> __device__ __forceinline__ R floor14(R x)
 {
-    return dmax<R>(x, FVB_LIT(R, 1e-14));
+    return smax<R>(x, FVB_LIT(R, 1e-14));
 }
 
 // Gas constants of one solver.  gm1 is formed as gamma - 1 at run time, the
@@ -256,9 +271,11 @@ __device__ __forceinline__ double snd_rsq_raw(double gp, double r)
     return gp * y;
 #endif
 }
+// (both sides evaluated and one selected: no branch)
 __device__ __forceinline__ double snd_rsq(double gp, double r)
 {
-    return gp > 1e-14 * r ? snd_rsq_raw(gp, r) : 1e-7;
+    const double c = snd_rsq_raw(gp, r);
+    return gp > 1e-14 * r ? c : 1e-7;
 }
 
 template <class R> struct GasF {
@@ -331,7 +348,7 @@ __device__ __forceinline__ void hll_fast(const R L[4], const R Rv[4], const GasF
     const R ER = pR * gs.igm1 + R(0.5) * rR * (uR * uR + tR * tR);
     // Einfeldt's form of the two-wave average: FL, FR or the subsonic
     // average without selects
-    const R SL = dmin<R>(dmin<R>(uL - cL, uR - cR), zero), SR = dmax<R>(dmax<R>(uL + cL, uR + cR), zero);
+    const R SL = smin<R>(smin<R>(uL - cL, uR - cR), zero), SR = smax<R>(smax<R>(uL + cL, uR + cR), zero);
     const R inv = frcp(SR - SL), SRL = SR * SL;
     const R mL = rL * uL, mR = rR * uR;
     Fh[0] = (SR * mL - SL * mR + SRL * (rR - rL)) * inv;
@@ -366,8 +383,8 @@ __device__ __forceinline__ void roe_fast(const R L[4], const R Rv[4], const GasF
     const R b4 = (dp + rr * c * dun) * (R(0.5) * ic2);
     // Harten-Hyman: |lambda| below eps/2 replaced by (lambda^2 + eps^2/4)/eps
     const R lam1 = a - c, lam4 = a + c;
-    const R eps1 = dmax<R>(zero, R(2) * ((uR - cR) - (uL - cL)));
-    const R eps4 = dmax<R>(zero, R(2) * ((uR + cR) - (uL + cL)));
+    const R eps1 = smax<R>(R(2) * ((uR - cR) - (uL - cL)), zero);
+    const R eps4 = smax<R>(R(2) * ((uR + cR) - (uL + cL)), zero);
     R al1 = dabs<R>(lam1), al4 = dabs<R>(lam4);
     const R al2 = dabs<R>(a);
     al1 = al1 < eps1 * R(0.5) ? (lam1 * lam1 + eps1 * eps1 * R(0.25)) * frcp(eps1) : al1;
@@ -407,7 +424,7 @@ __device__ __forceinline__ void recon_flux_fast(const R L[4], const R Rv[4], con
             cL = fsqrt(cs2L > FVB_LIT(R, 1e-14) ? cs2L : FVB_LIT(R, 1e-14));
             cR = fsqrt(cs2R > FVB_LIT(R, 1e-14) ? cs2R : FVB_LIT(R, 1e-14));
         }
-        const R SL = dmin<R>(uL - cL, uR - cR), SR = dmax<R>(uL + cL, uR + cR);
+        const R SL = smin<R>(uL - cL, uR - cR), SR = smax<R>(uL + cL, uR + cR);
         const R dL = rL * (SL - uL), dR = rR * (SR - uR);
         const R Ss = (pR - pL + dL * uL - dR * uR) * frcp(dL - dR);
         // side K: by the contact when subsonic, by the fan when supersonic
@@ -449,12 +466,12 @@ __device__ __forceinline__ void hlle_sensor_fast(const R WL[4], const R WR[4], R
     // Einfeldt's form: with SL- = min(SL, 0), SR+ = max(SR, 0) the HLL
     // average equals FL, FR or the subsonic average in the three wave
     // configurations, with no selects
-    const R SL = dmin<R>(dmin<R>(uL - cWL, uR - cWR), zero), SR = dmax<R>(dmax<R>(uL + cWL, uR + cWR), zero);
+    const R SL = smin<R>(smin<R>(uL - cWL, uR - cWR), zero), SR = smax<R>(smax<R>(uL + cWL, uR + cWR), zero);
     const R mL = rL * uL, mR = rR * uR;
     const R FL1 = mL * uL + pL, FR1 = mR * uR + pR;
     const R FL2 = mL * tL, FR2 = mR * tR;
     const R FL3 = (EWL + pL) * uL, FR3 = (EWR + pR) * uR;
-    const R dS = dmax<R>(SR - SL, FVB_LIT(R, 1e-10));
+    const R dS = smax<R>(SR - SL, FVB_LIT(R, 1e-10));
     const R dp = WR[3] - WL[3], ps = WR[3] + WL[3];
     const R dp2 = dp * dp;
     const R dd = dp2 + FVB_LIT(R, 0.1) * ps * ps;

@@ -152,6 +152,20 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
     } else {
         wait_box(t < ntiles ? start_single(t) : false);
     }
+    // which of this thread's conversion cells (k = tid + it NT) the HLLE
+    // reads the sound speed and energy of: the interior rows x columns
+    // [G-1, G+TX], and rows G-1, G+TY x the interior columns (the same cells
+    // in every tile, so the mask is formed once)
+    constexpr int NCV = (PL + NT - 1) / NT;
+    static_assert(NCV <= 32, "one mask bit per conversion cell");
+    unsigned cemask = 0;
+#pragma unroll
+    for (int it = 0; it < NCV; ++it) {
+        const int k = tid + it * NT, r = k / SW, c = k - r * SW;
+        const bool ce = ((unsigned)(r - G) < (unsigned)TY && (unsigned)(c - (G - 1)) < (unsigned)(TX + 2)) ||
+                        ((r == G - 1 || r == G + TY) && (unsigned)(c - G) < (unsigned)TX);
+        cemask |= (ce && k < PL ? 1u : 0u) << it;
+    }
     // single grid: the stage-3 wave-speed max is reduced once per CTA, and the
     // step control, the same for every tile, is read once (the leader is CTA
     // 0, whose first tile is tile 0)
@@ -184,16 +198,13 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
             break;
         }
         if (ctl.run && a.stage >= 0) {
-            for (int k = tid; k < PL; k += NT) {
+#pragma unroll
+            for (int it = 0; it < NCV; ++it) {
+                const int k = tid + it * NT;
+                if (k >= PL) break;
                 R w0 = IN[k], w1 = IN[PL + k], w2 = IN[2 * PL + k], w3 = IN[3 * PL + k];
-                // sound speed and energy only where the HLLE reads them: the
-                // interior rows x columns [G-1, G+TX], and rows G-1 and G+TY
-                // x the interior columns
-                const int r = k / SW, c = k - r * SW;
-                const bool ce = ((unsigned)(r - G) < (unsigned)TY && (unsigned)(c - (G - 1)) < (unsigned)(TX + 2)) ||
-                                ((r == G - 1 || r == G + TY) && (unsigned)(c - G) < (unsigned)TX);
                 if constexpr (FAST) {
-                    if (ce) {
+                    if ((cemask >> it) & 1u) {
                         R cc, ee;
                         cell_ce<R>(w0, w1, w2, w3, gf, cc, ee);
                         W[4 * PL + k] = cc;
