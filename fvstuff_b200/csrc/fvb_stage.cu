@@ -360,7 +360,8 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const __grid_constant__
                     } else {
                         lam = dabs<R>(w[1]) + dabs<R>(w[2]) + sound<R>(w[3], w[0], gs);
                     }
-                    lmax = fmax(lmax, (double)lam);
+                    // (a NaN lam is skipped, as fmax skips it; one compare-select)
+                    lmax = smax<double>((double)lam, lmax);
                 }
             }
         }
