@@ -49,8 +49,8 @@ __device__ void d2_hllc(double gam, const double UL[4], const double UR[4], doub
     double pL, cL, uL, vL, pR, cR, uR, vR;
     d2_prim(gam, UL[0], UL[1], UL[2], UL[3], pL, cL, uL, vL);
     d2_prim(gam, UR[0], UR[1], UR[2], UR[3], pR, cR, uR, vR);
-    const double SL = fmin(uL - cL, uR - cR);
-    const double SR = fmax(uL + cL, uR + cR);
+    const double SL = smin<double>(uL - cL, uR - cR);
+    const double SR = smax<double>(uL + cL, uR + cR);
     if (SL >= 0.0) {
         F[0] = UL[1]; F[1] = UL[1] * uL + pL; F[2] = UL[1] * vL; F[3] = (UL[3] + pL) * uL;
         return;
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(DNT, D2Shape<ORDER>::MINB)
             if (stage == 3) {
                 double p, cc, u, w;
                 d2_prim(gam, v[0], v[1], v[2], v[3], p, cc, u, w);
-                lacc = fmax(lacc, fabs(u) + fabs(w) + cc);  // lam_c, :362
+                lacc = smax<double>(fabs(u) + fabs(w) + cc, lacc);  // lam_c, :362
             }
         }
         if (stage == 3 && tid == 0 && t == 0) leader_finish<P64>(gd.ctrl);

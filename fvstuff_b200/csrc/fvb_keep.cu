@@ -31,12 +31,12 @@ __device__ __forceinline__ double k_snd(double rho, double p, double gam) { retu
 //                                              keep_fv_euler_2d.cu:99-132
 __device__ __forceinline__ void k_cell(const double U[4], double gam, double W[4], double Uf[4], double &s)
 {
-    double rho = fmax(U[0], KG_MIN), mx = U[1], my = U[2], E = U[3];
+    double rho = smax<double>(U[0], KG_MIN), mx = U[1], my = U[2], E = U[3];
     double u = mx / rho, v = my / rho;
     W[0] = rho;
     W[1] = mx / rho;
     W[2] = my / rho;
-    W[3] = fmax((gam - 1.) * (E - 0.5 * rho * (u * u + v * v)), KG_MIN);
+    W[3] = smax<double>((gam - 1.) * (E - 0.5 * rho * (u * u + v * v)), KG_MIN);
     Uf[0] = rho; Uf[1] = mx; Uf[2] = my; Uf[3] = E;
     s = log(W[3] / pow(W[0], gam));
 }
@@ -91,9 +91,9 @@ __device__ __forceinline__ void k_flux(const double WL[4], const double WR[4], c
     Fec[2] = Fc1 * ny + Fc2 * nx;
     Fec[3] = Fc3;
     const double rav = 0.5 * (rL + rR);
-    const double aav = k_snd(fmax(rav, KG_MIN), fmax(pb, KG_MIN), gam);
+    const double aav = k_snd(smax<double>(rav, KG_MIN), smax<double>(pb, KG_MIN), gam);
     const double l1 = fabs(unb - aav), l2 = fabs(unb), l3 = fabs(unb + aav);
-    const double lmin = fmin(l1, fmin(l2, l3)), lmax = fmax(l1, fmax(l2, l3));
+    const double lmin = smin<double>(l1, smin<double>(l2, l3)), lmax = smax<double>(l1, smax<double>(l2, l3));
     double aS = lmax;
     for (int q = 0; q < 4; ++q) {
         const double dU = UR[q] - UL[q];
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(KNT, 2) keep_stage_kernel(const GridDev gd, in
             k_flux(WL, WR, VLn, VRn, nx, ny, gam, fec, &aS);
             const double unL = WL[1] * nx + WL[2] * ny, unR = WR[1] * nx + WR[2] * ny;
             const double aR = k_snd(0.5 * (WL[0] + WR[0]), 0.5 * (WL[3] + WR[3]), gam);
-            const double lamt = fmax(fabs(unL), fabs(unR)) + aR;
+            const double lamt = smax<double>(fabs(unL), fabs(unR)) + aR;
             const double aJST = (1.0 / 32.0) * lamt;
             // entropy distance of the face                  keep_fv:249-258
             double ed = 0.;
@@ -276,14 +276,14 @@ __global__ void __launch_bounds__(KNT, 2) keep_stage_kernel(const GridDev gd, in
                 else if (stage == 2) v[q] = 0.75 * ua + 0.25 * ub + 0.25 * ctl.dt * L;
                 else v[q] = (1. / 3.) * ua + (2. / 3.) * ub + (2. / 3.) * ctl.dt * L;
             }
-            v[0] = fmax(v[0], KG_MIN);
-            v[3] = fmax(v[3], KG_MIN);
+            v[0] = smax<double>(v[0], KG_MIN);
+            v[3] = smax<double>(v[3], KG_MIN);
             put_cell<double>(gd, out, j, i, v);
             if (stage == 3) {
                 double Wn[4], Fn[4], sn;
                 k_cell(v, gam, Wn, Fn, sn);
                 const double cs = k_snd(Wn[0], Wn[3], gam);
-                lmax = fmax(lmax, (fabs(Wn[1]) + cs) + (fabs(Wn[2]) + cs));
+                lmax = smax<double>((fabs(Wn[1]) + cs) + (fabs(Wn[2]) + cs), lmax);
             }
         }
         if (stage == 3) {

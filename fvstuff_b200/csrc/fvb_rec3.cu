@@ -41,16 +41,16 @@ __device__ __forceinline__ double r3_snd(double rho, double p) { return sqrt(R3_
 // conserved point value -> floored primitives  fv_rec3_2d.cu:71-79
 __device__ __forceinline__ void r3_w(const double U[4], double W[4])
 {
-    const double r = fmax(U[0], R3_RHOFLOOR);
+    const double r = smax<double>(U[0], R3_RHOFLOOR);
     const double u = U[1] / r, v = U[2] / r;
     const double p = (R3_GAM - 1.0) * (U[3] - 0.5 * r * (u * u + v * v));
-    W[0] = r; W[1] = u; W[2] = v; W[3] = fmax(p, R3_PFLOOR);
+    W[0] = r; W[1] = u; W[2] = v; W[3] = smax<double>(p, R3_PFLOOR);
 }
 
 // pressure of a conserved state                fv_rec3_2d.cu:81-87
 __device__ __forceinline__ double r3_p(const double U[4])
 {
-    const double r = fmax(U[0], R3_RHOFLOOR);
+    const double r = smax<double>(U[0], R3_RHOFLOOR);
     const double u = U[1] / r, v = U[2] / r;
     return (R3_GAM - 1.0) * (U[3] - 0.5 * r * (u * u + v * v));
 }
@@ -66,7 +66,7 @@ __device__ void r3_hllc(const double L[4], const double R[4], double F[4])
     const double cL = r3_snd(rL, pL), cR = r3_snd(rR, pR);
     const double EL = pL / (R3_GAM - 1.) + 0.5 * rL * (uL * uL + tL * tL);
     const double ER = pR / (R3_GAM - 1.) + 0.5 * rR * (uR * uR + tR * tR);
-    const double SL = fmin(uL - cL, uR - cR), SR = fmax(uL + cL, uR + cR);
+    const double SL = smin<double>(uL - cL, uR - cR), SR = smax<double>(uL + cL, uR + cR);
     const double FL[4] = {rL * uL, rL * uL * uL + pL, rL * uL * tL, (EL + pL) * uL};
     const double FR[4] = {rR * uR, rR * uR * uR + pR, rR * uR * tR, (ER + pR) * uR};
     if (SL >= 0.) { for (int q = 0; q < 4; q++) F[q] = FL[q]; return; }
@@ -95,7 +95,7 @@ __device__ __forceinline__ void r3_scale_w(const double Ub[4], double U[4], doub
         const double th = (d > 0.) ? (Ub[0] - R3_RHOFLOOR) / d : 0.;
         for (int q = 0; q < 4; q++) U[q] = Ub[q] + th * (U[q] - Ub[q]);
     }
-    double r = fmax(U[0], R3_RHOFLOOR);
+    double r = smax<double>(U[0], R3_RHOFLOOR);
     double u = U[1] / r, v = U[2] / r;
     double p = (R3_GAM - 1.0) * (U[3] - 0.5 * r * (u * u + v * v));
     if (p < R3_PFLOOR) {
@@ -108,12 +108,12 @@ __device__ __forceinline__ void r3_scale_w(const double Ub[4], double U[4], doub
             else hi = mid;
         }
         for (int q = 0; q < 4; q++) U[q] = Ub[q] + lo * (U[q] - Ub[q]);
-        r = fmax(U[0], R3_RHOFLOOR);
+        r = smax<double>(U[0], R3_RHOFLOOR);
         u = U[1] / r;
         v = U[2] / r;
         p = (R3_GAM - 1.0) * (U[3] - 0.5 * r * (u * u + v * v));
     }
-    W[0] = r; W[1] = u; W[2] = v; W[3] = fmax(p, R3_PFLOOR);
+    W[0] = r; W[1] = u; W[2] = v; W[3] = smax<double>(p, R3_PFLOOR);
 }
 
 // 2x2-block limiter on U[c][q] (cells c = 0..3: (i0,j0), (i0+1,j0),
@@ -127,10 +127,10 @@ __device__ bool r3_limit_block(double U[4][4], int *brutal)
     const double pb = r3_p(Ub);
     if (Ub[0] < R3_RHOFLOOR || pb < R3_PFLOOR) {
         ++*brutal;
-        const double rb = fmax(Ub[0], 10. * R3_RHOFLOOR);
+        const double rb = smax<double>(Ub[0], 10. * R3_RHOFLOOR);
         const double Efix = (10. * R3_PFLOOR) / (R3_GAM - 1.) + 0.5 * (Ub[1] * Ub[1] + Ub[2] * Ub[2]) / rb;
         Ub[0] = rb;
-        Ub[3] = fmax(Ub[3], Efix);
+        Ub[3] = smax<double>(Ub[3], Efix);
     }
     double C[4][4];
     for (int q = 0; q < 4; q++) {
@@ -143,7 +143,7 @@ __device__ bool r3_limit_block(double U[4][4], int *brutal)
     for (int c = 0; c < 4; c++)
         if (C[c][0] < R3_RHOFLOOR) {
             const double d = Ub[0] - C[c][0];
-            if (d > 0.) th = fmin(th, (Ub[0] - R3_RHOFLOOR) / d);
+            if (d > 0.) th = smin<double>((Ub[0] - R3_RHOFLOOR) / d, th);
         }
     if (th < 1.)
         for (int c = 0; c < 4; c++)
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(RNT, 2) rec3_stage_kernel(const GridDev gd, in
                 if (stage == 3) {
                     double W[4];
                     r3_w(U[cc], W);
-                    lacc = fmax(lacc, fabs(W[1]) + fabs(W[2]) + r3_snd(W[0], W[3]));
+                    lacc = smax<double>(fabs(W[1]) + fabs(W[2]) + r3_snd(W[0], W[3]), lacc);
                 }
             }
         }
