@@ -92,9 +92,13 @@ struct StageArgs {
 struct TileShape {
     int tx, ty, nt;
 };
-constexpr int kNumTileShapes = 6;
+constexpr int kNumTileShapes = 7;
 constexpr TileShape kTileShapes[kNumTileShapes] = {
-    {32, 15, 256}, {32, 7, 128}, {64, 7, 256}, {16, 15, 256}, {32, 9, 256}, {32, 16, 256}};
+    {32, 15, 256}, {32, 7, 128}, {64, 7, 256}, {16, 15, 256}, {32, 9, 256}, {32, 16, 256}, {32, 14, 256}};
+// the variant whose FP32-compensated kernel evaluates faces and cells as
+// pairs of rows TY/2 apart (fvb_stage32c.cu, stage32p_kernel); the FP64 and
+// FP32 kernels treat it as one more tile shape
+constexpr int kRowPairShape = 6;
 
 // TMA descriptors (fvb_stage.cu): encode the four maps of a grid for a
 // tile shape into host memory; false if this grid cannot use TMA

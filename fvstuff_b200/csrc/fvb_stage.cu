@@ -439,10 +439,11 @@ static KernelEntry entry32c(int shape)
 }
 
 #define FVB_SHAPES(P, O) \
-    entry<P, O, 0>(), entry<P, O, 1>(), entry<P, O, 2>(), entry<P, O, 3>(), entry<P, O, 4>(), entry<P, O, 5>()
+    entry<P, O, 0>(), entry<P, O, 1>(), entry<P, O, 2>(), entry<P, O, 3>(), entry<P, O, 4>(), entry<P, O, 5>(), \
+        entry<P, O, 6>()
 #define FVB_SHAPES_RS(RS) \
     entry<P64, 7, 0, RS>(), entry<P64, 7, 1, RS>(), entry<P64, 7, 2, RS>(), entry<P64, 7, 3, RS>(), \
-        entry<P64, 7, 4, RS>(), entry<P64, 7, 5, RS>()
+        entry<P64, 7, 4, RS>(), entry<P64, 7, 5, RS>(), entry<P64, 7, 6, RS>()
 
 static KernelEntry *table_for(int prec, int order, int rs = 0)
 {
@@ -455,7 +456,8 @@ static KernelEntry *table_for(int prec, int order, int rs = 0)
     static KernelEntry t64_3[] = {FVB_SHAPES(P64, 3)};
     static KernelEntry t64_9[] = {FVB_SHAPES(P64, 9)};
     static KernelEntry t32_7[] = {FVB_SHAPES(P32, 7)};
-    static KernelEntry t32c_7[] = {entry32c(0), entry32c(1), entry32c(2), entry32c(3), entry32c(4), entry32c(5)};
+    static KernelEntry t32c_7[] = {entry32c(0), entry32c(1), entry32c(2), entry32c(3), entry32c(4), entry32c(5),
+                                   entry32c(6)};
     if (prec == P64)
         return order == 7 ? t64_7 : order == 5 ? t64_5 : order == 3 ? t64_3 : order == 9 ? t64_9 : nullptr;
     if (order != 7) return nullptr;

@@ -57,7 +57,7 @@ def test_f32c_kh_short_against_f64():
     assert e[0] <= 1e-6
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5, 6])
 def test_f32c_tile_variants_against_f64(tile):
     """Every tile variant of the compensated kernel, on a ragged grid with
     reflecting walls (ghost images with negated momenta on all four sides)."""

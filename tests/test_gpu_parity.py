@@ -198,7 +198,7 @@ def test_orders_step_f64_matches_oracle(order, bc, n, case):
     _step_against_oracle(bc, n, case, order)
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5, 6])
 def test_tile_variants_agree(tile):
     n = 70
     U = _padded(riemann4(n, seed=5), 1)
