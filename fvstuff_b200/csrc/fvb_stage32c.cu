@@ -120,6 +120,22 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
         }
         __syncthreads();
     };
+    // The wait at the end of a tile needs no block barrier when the box came
+    // through TMA: the next writes of every buffer are already ordered by
+    // the barriers inside the tile (W by the conversion barrier, FX / FY by
+    // the face barrier the update follows, IN by the conversion barrier the
+    // next load is issued behind; the update reads neither W nor IN), and
+    // each thread's own wait makes the box visible to it.  A box loaded by
+    // the threads themselves needs the barrier.  A timeout is agreed on at
+    // the next conversion barrier.
+    auto wait_box_own = [&](bool tma) {
+        if (tma) {
+            if (mbar_wait(&s_bar, phase)) phase ^= 1;
+            else s_err = 1;
+        } else {
+            __syncthreads();
+        }
+    };
     // single grid: start the halo-box load of tile t (every thread: the
     // plain path loads cooperatively)
     auto start_single = [&](int t) -> bool {
@@ -185,10 +201,6 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
         const int n = gd.n;
         const int tx0 = (tile % gd.tiles_x) * TX, ty0 = (tile / gd.tiles_x) * TY;
         const float gam = (float)gd.gam, gm1 = (float)gd.gam - 1.0f, igm1 = (float)(1.0 / (gd.gam - 1.0));
-        if (s_err) {
-            if (tid == 0 && gd.ctrl) gd.ctrl->status = FVB_ERR_TIMEOUT;
-            break;
-        }
         // ---- 1. stage input U0 + d into W as primitives (+ c, E where the
         //         HLLE reads them, cemask) ------------------------------------
         if (ctl.run) {
@@ -215,6 +227,12 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
             }
         }
         __syncthreads();
+        // a halo load that never arrived (seen by any thread): record it and
+        // stop; every thread reads s_err after the same barrier
+        if (s_err) {
+            if (tid == 0 && gd.ctrl) gd.ctrl->status = FVB_ERR_TIMEOUT;
+            break;
+        }
         // ---- 2. load the next tile into IN (asynchronous through TMA) -------
         // (in a batched launch warp 0 also fetches that tile's header)
         bool next_tma = false;
@@ -319,8 +337,8 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32c_kernel(const
                 lacc = fmax(lacc, (double)lmax);
             }
         }
-        // ---- 6. next tile's halo box: wait, then release W / FX / FY --------
-        wait_box(next_tma);
+        // ---- 6. next tile's halo box -----------------------------------------
+        wait_box_own(next_tma);
     }
     if (!batched && a.stage == 3) {
 #pragma unroll
@@ -409,6 +427,22 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32p_kernel(const
         }
         __syncthreads();
     };
+    // The wait at the end of a tile needs no block barrier when the box came
+    // through TMA: the next writes of every buffer are already ordered by
+    // the barriers inside the tile (W by the conversion barrier, FX / FY by
+    // the face barrier the update follows, IN by the conversion barrier the
+    // next load is issued behind; the update reads neither W nor IN), and
+    // each thread's own wait makes the box visible to it.  A box loaded by
+    // the threads themselves needs the barrier.  A timeout is agreed on at
+    // the next conversion barrier.
+    auto wait_box_own = [&](bool tma) {
+        if (tma) {
+            if (mbar_wait(&s_bar, phase)) phase ^= 1;
+            else s_err = 1;
+        } else {
+            __syncthreads();
+        }
+    };
     auto start_single = [&](int t) -> bool {
         if (tid == 0 && a.grid.tmap) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         issue_tile_load<P32C, G, SW, SH, NT>(a.grid, a.stage, cur, t, IN, &s_bar, tid);
@@ -463,10 +497,6 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32p_kernel(const
         const int n = gd.n;
         const int tx0 = (tile % gd.tiles_x) * TX, ty0 = (tile / gd.tiles_x) * TY;
         const float gam = (float)gd.gam, gm1 = (float)gd.gam - 1.0f, igm1 = (float)(1.0 / (gd.gam - 1.0));
-        if (s_err) {
-            if (tid == 0 && gd.ctrl) gd.ctrl->status = FVB_ERR_TIMEOUT;
-            break;
-        }
         // ---- 1. stage input U0 + d into W2 as primitive row pairs (+ c, E
         //         where the HLLE reads them) -----------------------------------
         if (ctl.run) {
@@ -500,6 +530,12 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32p_kernel(const
             }
         }
         __syncthreads();
+        // a halo load that never arrived (seen by any thread): record it and
+        // stop; every thread reads s_err after the same barrier
+        if (s_err) {
+            if (tid == 0 && gd.ctrl) gd.ctrl->status = FVB_ERR_TIMEOUT;
+            break;
+        }
         // ---- 2. load the next tile into IN (asynchronous through TMA) -------
         bool next_tma = false;
         if (has_next) {
@@ -622,8 +658,8 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32p_kernel(const
                 lacc = fmax(lacc, (double)lmax);
             }
         }
-        // ---- 6. next tile's halo box: wait, then release W2 / FX2 / FY2 -----
-        wait_box(next_tma);
+        // ---- 6. next tile's halo box -----------------------------------------
+        wait_box_own(next_tma);
     }
     if (!batched && a.stage == 3) {
 #pragma unroll
