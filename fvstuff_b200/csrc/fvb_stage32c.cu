@@ -427,14 +427,8 @@ __global__ void __launch_bounds__(NT, MinBlocks32c<NT>::v) stage32p_kernel(const
         }
         __syncthreads();
     };
-    // The wait at the end of a tile needs no block barrier when the box came
-    // through TMA: the next writes of every buffer are already ordered by
-    // the barriers inside the tile (W by the conversion barrier, FX / FY by
-    // the face barrier the update follows, IN by the conversion barrier the
-    // next load is issued behind; the update reads neither W nor IN), and
-    // each thread's own wait makes the box visible to it.  A box loaded by
-    // the threads themselves needs the barrier.  A timeout is agreed on at
-    // the next conversion barrier.
+    // end-of-tile wait without a block barrier for a TMA-fed box, as in
+    // stage32c_kernel (W2 / FX2 / FY2 in place of W / FX / FY)
     auto wait_box_own = [&](bool tma) {
         if (tma) {
             if (mbar_wait(&s_bar, phase)) phase ^= 1;
