@@ -137,6 +137,37 @@ def test_batch_instances_match_alone(prec):
     assert b.bytes_in_use() == 0
 
 
+def test_batch_row_pair_variant_matches_alone():
+    """The FP32c row-pair kernel (tile variant 6, used only when asked for)
+    in a batch of ragged grids, bit for bit against each grid run alone with
+    the same variant, and against variant 5 alone (the two kernels evaluate
+    the same operations in the same order)."""
+    sizes = [64, 33, 96, 50]
+    b = F.Batch(precision="f32c", tile=6)
+    ids, cases = [], []
+    for k, n in enumerate(sizes):
+        d, c = _desc(n, 200 + k, 0.04)
+        ids.append(b.add(d))
+        cases.append((n, c, d.t_end))
+    done = set()
+    for _ in range(400):
+        b.run(8)
+        done.update(b.poll())
+        if len(done) == len(sizes):
+            break
+    assert done == set(ids)
+    for iid, (n, c, t_end) in zip(ids, cases):
+        st = b.stats(iid)
+        assert st.status == 0
+        got = b.get_state(iid, n)
+        for tile in (6, 5):
+            s = F.Solver(n, precision="f32c", bc="transmissive", cfl=0.5, tile=tile)
+            s.init_case(c)
+            s.advance(t_end)
+            assert s.sync().steps == st.steps
+            assert np.array_equal(got, s.get_state(interior=True)), (iid, n, tile)
+
+
 def test_batch_join_midway_and_budget():
     b = F.Batch(precision="f32c", hbm_budget=F.Batch(precision="f32c").instance_bytes(64) * 2)
     d1, _ = _desc(64, 1, 0.04)
